@@ -1,0 +1,283 @@
+"""Python binding of the C ABI in include/fsmeld_cuda.h (ctypes).
+
+Mirrors the reference's entry points (include/funcs.h:64-72) by name and
+argument meaning:
+
+    FSMELD(target_path, query_path, m, cutoff, tag, w, arg, exclude_start=-1, exclude_end=-1)
+    FSMELD_find_threshold(target_path, query_path, m, threshold, tag, w, arg, top_k, ...)
+    FSMELD_exact(target_path, query_path, m, cutoff, tag, w, arg, top_k=0, ...)
+
+which print the reference's output, and an in-memory `Engine` for callers
+that hold the target and query as arrays.  Errors raise `FsmeldError` with
+the library's message, as the reference raises std::runtime_error /
+std::invalid_argument.  There is no CPU fallback: importing without the
+built library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "lib", "libfsmeld_cuda.so")
+CLI_PATH = os.path.join(_PKG, "bin", "fsmeld")
+
+METRICS = {"dtw": 1, "edr": 2, "erp": 3, "lcss": 4, "msm": 5}
+OK, E_ARG, E_CUDA, E_NOMEM, E_SHORT, E_FEWER_K, E_UNSUPPORTED, E_IO = 0, -1, -2, -3, -4, -5, -6, -7
+
+
+class FsmeldError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(message)
+        self.status = status
+
+
+class Counters(C.Structure):
+    _fields_ = [("valid", C.c_int64), ("invalid", C.c_int64), ("after_lb", C.c_int64),
+                ("after_glb", C.c_int64), ("exact_evals", C.c_int64), ("matches", C.c_int64),
+                ("threshold", C.c_double), ("m_k", C.c_int32), ("reserved", C.c_int32),
+                ("segments", C.c_int64), ("tail", C.c_int64), ("device_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class Query(C.Structure):
+    _fields_ = [("query", C.POINTER(C.c_double)), ("m", C.c_int32), ("metric", C.c_int32),
+                ("w", C.c_int32), ("k", C.c_int32), ("arg", C.c_double), ("cutoff", C.c_double),
+                ("exclude_begin", C.c_int64), ("exclude_end", C.c_int64)]
+
+
+class Result(C.Structure):
+    _fields_ = [("idx", C.POINTER(C.c_int64)), ("dist", C.POINTER(C.c_double)),
+                ("capacity", C.c_int64), ("count", C.c_int64), ("status", C.c_int32),
+                ("reserved", C.c_int32), ("counters", Counters),
+                ("seg_counts", C.POINTER(C.c_int64))]
+
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library (built in-tree by fsmeld_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FsmeldError(E_CUDA, f"CUDA library not built: {LIB_PATH} (run python -m fsmeld_b200.build)")
+        L = C.CDLL(LIB_PATH)
+        dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int64)
+        ctxp = C.c_void_p
+        sig = {
+            "fsmeld_open": (C.c_int, [C.c_int, dp, C.c_int64, C.POINTER(ctxp)]),
+            "fsmeld_open_file": (C.c_int, [C.c_int, C.c_char_p, C.POINTER(ctxp)]),
+            "fsmeld_open_device": (C.c_int, [C.c_int, C.c_void_p, C.c_int64, C.POINTER(ctxp)]),
+            "fsmeld_close": (C.c_int, [ctxp]),
+            "fsmeld_target_length": (C.c_int64, [ctxp]),
+            "fsmeld_last_error": (C.c_char_p, [ctxp]),
+            "fsmeld_strerror": (C.c_char_p, [C.c_int]),
+            "fsmeld_set_workspace_limit": (C.c_int, [ctxp, C.c_int64]),
+            "fsmeld_kernel_launches": (C.c_int64, [ctxp]),
+            "fsmeld_search": (C.c_int, [ctxp, dp, C.c_int, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int64,
+                                        C.c_int64, ip, C.c_int64, ip, C.POINTER(Counters), ip]),
+            "fsmeld_cutoff": (C.c_int, [ctxp, dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int64,
+                                        C.c_int64, ip, dp, C.POINTER(Counters)]),
+            "fsmeld_exact": (C.c_int, [ctxp, dp, C.c_int, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int64,
+                                       C.c_int64, ip, dp, C.c_int64, ip, C.POINTER(Counters)]),
+            "fsmeld_batch": (C.c_int, [ctxp, C.c_int, C.POINTER(Query), C.c_int, C.POINTER(Result)]),
+            "fsmeld_inspect": (C.c_int64, [ctxp, dp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, dp,
+                                           C.c_int64]),
+            "fsmeld_search_file": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_double, C.c_char_p, C.c_int,
+                                             C.c_double, C.c_int64, C.c_int64]),
+            "fsmeld_cutoff_file": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_char_p, C.c_int,
+                                             C.c_double, C.c_int64, C.c_int64]),
+            "fsmeld_exact_file": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_double, C.c_char_p, C.c_int,
+                                            C.c_double, C.c_int64, C.c_int64]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    """Names of the C ABI entry points declared in include/fsmeld_cuda.h."""
+    return ["fsmeld_open", "fsmeld_open_file", "fsmeld_open_device", "fsmeld_close", "fsmeld_target_length",
+            "fsmeld_last_error", "fsmeld_strerror", "fsmeld_set_workspace_limit", "fsmeld_kernel_launches",
+            "fsmeld_search", "fsmeld_cutoff", "fsmeld_exact", "fsmeld_batch", "fsmeld_inspect",
+            "fsmeld_search_file", "fsmeld_cutoff_file", "fsmeld_exact_file"]
+
+
+def _check(status, ctx=None):
+    if status != OK:
+        msg = lib().fsmeld_last_error(ctx).decode(errors="replace") or lib().fsmeld_strerror(status).decode()
+        raise FsmeldError(status, msg)
+
+
+def _metric(tag):
+    if isinstance(tag, int):
+        return tag
+    if tag not in METRICS:
+        raise FsmeldError(E_ARG, f"Unsupported metric: {tag}")
+    return METRICS[tag]
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _iptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int64))
+
+
+class Engine:
+    """A target series resident on one GPU, queried through the C ABI."""
+
+    def __init__(self, target=None, *, path=None, device=0, device_ptr=None, n=None):
+        self._ctx = C.c_void_p()
+        L = lib()
+        if path is not None:
+            _check(L.fsmeld_open_file(device, os.fsencode(path), C.byref(self._ctx)))
+        elif device_ptr is not None:
+            _check(L.fsmeld_open_device(device, C.c_void_p(device_ptr), int(n), C.byref(self._ctx)))
+        else:
+            t = np.ascontiguousarray(target, dtype=np.float64)
+            _check(L.fsmeld_open(device, _dptr(t), len(t), C.byref(self._ctx)))
+        self.n = L.fsmeld_target_length(self._ctx)
+
+    def close(self):
+        if self._ctx:
+            lib().fsmeld_close(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def launches(self):
+        return lib().fsmeld_kernel_launches(self._ctx)
+
+    def set_workspace_limit(self, nbytes):
+        _check(lib().fsmeld_set_workspace_limit(self._ctx, int(nbytes)), self._ctx)
+
+    def search(self, query, m, cutoff, metric, w, arg=0.0, exclude=(-1, -1), seg_counts=False):
+        q = np.ascontiguousarray(query[:m], dtype=np.float64)
+        cap = 1 << 16
+        cnt = Counters()
+        nseg = max(1, (self.n - m + 1) // _kml(m, self.n))
+        segs = np.zeros(3 * nseg, dtype=np.int64) if seg_counts else None
+        while True:
+            idx = np.zeros(cap, dtype=np.int64)
+            count = C.c_int64(0)
+            st = lib().fsmeld_search(self._ctx, _dptr(q), m, float(cutoff), _metric(metric), w, float(arg),
+                                     exclude[0], exclude[1], _iptr(idx), cap, C.byref(count), C.byref(cnt),
+                                     _iptr(segs) if segs is not None else None)
+            _check(st, self._ctx)
+            if count.value <= cap:
+                res = (idx[:count.value].copy(), cnt.as_dict())
+                return res + ((segs.reshape(-1, 3),) if seg_counts else ())
+            cap = count.value
+
+    def cutoff(self, query, m, k, metric, w, arg=0.0, exclude=(-1, -1)):
+        q = np.ascontiguousarray(query[:m], dtype=np.float64)
+        idx = np.zeros(k, dtype=np.int64)
+        dist = np.zeros(k)
+        cnt = Counters()
+        _check(lib().fsmeld_cutoff(self._ctx, _dptr(q), m, k, _metric(metric), w, float(arg), exclude[0],
+                                   exclude[1], _iptr(idx), _dptr(dist), C.byref(cnt)), self._ctx)
+        return idx, dist, cnt.as_dict()
+
+    def exact(self, query, m, cutoff, metric, w, arg=0.0, exclude=(-1, -1)):
+        q = np.ascontiguousarray(query[:m], dtype=np.float64)
+        cap = 1 << 16
+        cnt = Counters()
+        while True:
+            idx = np.zeros(cap, dtype=np.int64)
+            dist = np.zeros(cap)
+            count = C.c_int64(0)
+            _check(lib().fsmeld_exact(self._ctx, _dptr(q), m, float(cutoff), _metric(metric), w, float(arg),
+                                      exclude[0], exclude[1], _iptr(idx), _dptr(dist), cap, C.byref(count),
+                                      C.byref(cnt)), self._ctx)
+            if count.value <= cap:
+                return idx[:count.value].copy(), dist[:count.value].copy(), cnt.as_dict()
+            cap = count.value
+
+    def batch(self, mode, queries, capacity=1 << 14):
+        """queries: list of dicts with query, m, metric, w, arg, cutoff or k, exclude."""
+        mode_id = {"search": 0, "cutoff": 1, "exact": 2}[mode]
+        n = len(queries)
+        qs = (Query * n)()
+        rs = (Result * n)()
+        keep = []
+        for i, d in enumerate(queries):
+            q = np.ascontiguousarray(d["query"][:d["m"]], dtype=np.float64)
+            cap = d.get("k", capacity) if mode == "cutoff" else capacity
+            idx = np.zeros(cap, dtype=np.int64)
+            dist = np.zeros(cap)
+            keep += [q, idx, dist]
+            ex = d.get("exclude", (-1, -1))
+            qs[i] = Query(_dptr(q), d["m"], _metric(d["metric"]), d["w"], d.get("k", 0), float(d.get("arg", 0.0)),
+                          float(d.get("cutoff", 0.0)), ex[0], ex[1])
+            rs[i].idx = _iptr(idx)
+            rs[i].dist = _dptr(dist)
+            rs[i].capacity = cap
+        st = lib().fsmeld_batch(self._ctx, mode_id, qs, n, rs)
+        out = []
+        for i in range(n):
+            r = rs[i]
+            idx, dist = keep[3 * i + 1], keep[3 * i + 2]
+            c = min(r.count, r.capacity)
+            out.append({"status": r.status, "idx": idx[:c].copy(), "dist": dist[:c].copy(), "count": r.count,
+                        "counters": r.counters.as_dict()})
+        if st not in (OK,) and all(o["status"] == OK for o in out):
+            _check(st, self._ctx)
+        return out
+
+    def inspect(self, query, m, metric, w, arg, what):
+        q = np.ascontiguousarray(query[:m], dtype=np.float64)
+        n = lib().fsmeld_inspect(self._ctx, _dptr(q), m, _metric(metric), w, float(arg), what, None, 0)
+        if n < 0:
+            _check(int(n), self._ctx)
+        out = np.zeros(n)
+        lib().fsmeld_inspect(self._ctx, _dptr(q), m, _metric(metric), w, float(arg), what, _dptr(out), n)
+        return out
+
+
+def _kml(m, n):
+    sel = 1
+    while sel < 8 * m:
+        sel *= 2
+    sel = min(sel, n)
+    return sel - m + 1
+
+
+# ---- reference-named entry points (print the reference's output) -------------
+
+def FSMELD(bi_t, bi_q, m, threshold, tag, w, arg, exclude_start=-1, exclude_end=-1):
+    _check(lib().fsmeld_search_file(os.fsencode(bi_t), os.fsencode(bi_q), m, float(threshold), tag.encode(), w,
+                                    float(arg), exclude_start, exclude_end))
+
+
+def FSMELD_find_threshold(bi_t, bi_q, m, threshold, tag, w, arg, top_k, exclude_start=-1, exclude_end=-1):
+    del threshold  # the reference passes DBL_MAX here (src/main.cpp:95)
+    _check(lib().fsmeld_cutoff_file(os.fsencode(bi_t), os.fsencode(bi_q), m, int(top_k), tag.encode(), w,
+                                    float(arg), exclude_start, exclude_end))
+
+
+def FSMELD_exact(bi_t, bi_q, m, threshold, tag, w, arg, top_k=0, exclude_start=-1, exclude_end=-1):
+    if top_k:
+        raise FsmeldError(E_UNSUPPORTED, "exact top-k derivation is not exposed by the command line")
+    _check(lib().fsmeld_exact_file(os.fsencode(bi_t), os.fsencode(bi_q), m, float(threshold), tag.encode(), w,
+                                   float(arg), exclude_start, exclude_end))

@@ -1,0 +1,118 @@
+// Shared definitions for the FSMELD sm_100a kernels.
+//
+// Bit-exactness: every stage whose bits decide a match (window statistics,
+// candidate z-normalisation, GLB, the elastic DPs, the threshold sweep) uses
+// explicit round-to-nearest intrinsics (__dadd_rn, __dmul_rn, ...), which the
+// compiler never contracts into fused multiply-adds, so each operation rounds
+// exactly as the reference's scalar C++ does.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fsm {
+
+constexpr double kDpMax = 1e18;                     // src/ElasticMeasures.cpp:7
+constexpr double kGlbMax = (double)1008610086;      // include/def.h:7
+constexpr double kSigmaFloor = 1e-12;               // src/fsmeld.cpp:126,129
+constexpr double kLbTol = 1e-9;                     // include/fsmeld_internal.h:10
+
+enum Metric : int { DTW = 1, EDR = 2, ERP = 3, LCSS = 4, MSM = 5 };
+
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double dsqrt(double a) { return __dsqrt_rn(a); }
+__device__ __forceinline__ double dnan() { return __longlong_as_double(0x7ff8000000000000LL); }
+__device__ __forceinline__ double dsq(double a, double b) { double d = dsub(a, b); return dmul(d, d); }
+// std::max(0.0, x): (0.0 < x) ? x : 0.0 (a NaN x gives 0.0)
+__device__ __forceinline__ double dmax0(double x) { return (0.0 < x) ? x : 0.0; }
+// std::min({a, b, c}) for non-NaN operands
+__device__ __forceinline__ double dmin3(double a, double b, double c) {
+    double r = a;
+    if (b < r) r = b;
+    if (c < r) r = c;
+    return r;
+}
+
+// Macro-segment geometry of one (target, m) pair (src/fsmeld.cpp:28-37,
+// 647-661): segment s < forsize starts at s*kml; the last segment (when
+// tail > 0) is the EOF-aligned tail whose processed windows are
+// [tail_lo, kml).  Window j of segment s has global index s*kml + j - lo(s),
+// which is also its start position in the target.
+struct Geom {
+    long long n;
+    int m, m_k, kml;
+    int tail_lo;           // kml - tail (== kml when there is no tail)
+    long long forsize, S;  // full segments; total segments including the tail
+    long long tsn;         // n - m + 1 windows
+    long long excl_b, excl_e;
+    __host__ __device__ long long off(long long s) const { return s < forsize ? s * kml : n - m_k; }
+    __host__ __device__ int lo(long long s) const { return s < forsize ? 0 : tail_lo; }
+    __host__ __device__ long long gidx(long long s, int j) const { return s * kml + (j - lo(s)); }
+    // statistics row/column of global window g
+    __host__ __device__ void locate(long long g, long long* s, int* j) const {
+        long long q = g / kml;
+        if (q < forsize) { *s = q; *j = (int)(g - q * kml); }
+        else { *s = forsize; *j = tail_lo + (int)(g - forsize * kml); }
+    }
+    __host__ __device__ bool excluded(long long g) const {
+        return excl_b >= 0 && excl_e > excl_b && g >= excl_b && g < excl_e;
+    }
+};
+
+// src/fsmeld.cpp:126 (with mvmean's NaN for non-finite windows) and the
+// exclusion interval of src/fsmeld.cpp:139-152.
+__device__ __forceinline__ bool window_invalid(double sigma, const Geom& g, long long gi) {
+    return !(isfinite(sigma) && sigma > kSigmaFloor) || g.excluded(gi);
+}
+
+// include/fsmeld_internal.h:9-19: prune only bounds that exceed the cutoff by
+// more than the FFT round-off guard.
+__device__ __forceinline__ bool lbip_exceeds(double bound, double cutoff, int metric) {
+    if (!isfinite(bound) || !(bound > dadd(cutoff, kLbTol))) return false;
+    if (metric == DTW || metric == ERP) {
+        const double limit = dadd(cutoff, kLbTol);
+        return bound > dsqrt(dadd(dmul(limit, limit), kLbTol));
+    }
+    return true;
+}
+
+// Per-query tables prepared on the host (query z-normalisation as
+// src/fsmeld.cpp:622-643, powers with the C library's pow as
+// src/find_t_lp.cpp:253 etc.).
+struct QueryDev {
+    int m, w, metric, p;
+    double arg;
+    double cutoff;
+    const double* qn;      // normalised query, original order [m]
+    const double* LQ;      // query envelope (radius w) [m]
+    const double* UQ;
+    const double* qs;      // sorted ascending [m]
+    const double* pw;      // pow(qs[j], a) for a = 0,1,2: [3][m]
+    const double* Dq;      // D(qs[j]) [m]   (src/find_t_lp.cpp:148-159)
+    const double* tlq;     // t_l(qs[j]) [m] (src/find_t_lp.cpp:177-186)
+    const double* tuq;     // t_u(qs[j]) [m] (src/find_t_lp.cpp:167-176)
+    // ERP (src/find_t_lp.cpp:510-654): tables by original query index
+    const double* opw;     // pow(qn[i], a): [3][m]
+    const double* oD;      // D(qn[i]) [m]
+    const double* otl;     // t_l(qn[i]) [m]
+    const double* otu;     // t_u(qn[i]) [m]
+    const int* ordA_l;     // H2 pop order, lower side: t_l desc, index asc
+    const int* ordB_l;     // H1 pop order, lower side: q desc
+    const int* ordA_u;     // H2 pop order, upper side: t_u asc, index asc
+    const int* ordB_u;     // H1 pop order, upper side: q asc
+};
+
+}  // namespace fsm
+
+#define FSM_CUDA_TRY(expr)                                                        \
+    do {                                                                          \
+        cudaError_t _e = (expr);                                                  \
+        if (_e != cudaSuccess) return ::fsm::cuda_fail(_e, #expr, __FILE__, __LINE__); \
+    } while (0)
+
+namespace fsm {
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
+}

@@ -1,0 +1,995 @@
+// Host orchestration of the FSMELD pipeline on one GPU, behind the C ABI in
+// include/fsmeld_cuda.h.
+//
+// Per query: window statistics (k_mvmean) -> envelopes (k_envelope) ->
+// thresholds (k_threshold) -> LB_IP + compaction (k_lbip) -> GLB
+// (k_glb_tq, k_glb_qt) -> exact DP (k_dp) -> ordered results.  Statistics
+// and envelopes depend only on (target, m, w), so a batch computes them once
+// per distinct (m, w).  All candidate lists stay on the device; the host
+// reads back counters and the final (small) result lists.
+//
+// The host prepares each query exactly as the reference does
+// (src/fsmeld.cpp:622-643: sequential sums, mean, sigma, (q - mean) / sigma;
+// sorted copy; pow(q, a) from the C library as src/find_t_lp.cpp:253) and
+// uploads the tables the kernels read.
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/fsmeld_cuda.h"
+#include "common.cuh"
+#include "engine.h"
+#include "kernels.cuh"
+
+namespace fsm {
+
+thread_local std::string g_last_error;
+
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
+    char buf[512];
+    snprintf(buf, sizeof(buf), "CUDA error %s (%s) at %s:%d: %s", cudaGetErrorName(e),
+             cudaGetErrorString(e), file, line, what);
+    g_last_error = buf;
+    return e == cudaErrorMemoryAllocation ? FSMELD_E_NOMEM : FSMELD_E_CUDA;
+}
+
+static int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+// ------------------------------------------------------------------ geometry
+
+// src/fsmeld.cpp:28-37
+int macro_length(int m, long long available) {
+    long long sel = 1;
+    while (sel < 8LL * m) sel *= 2;
+    if (available < 2LL * m - 1) return -1;
+    if (available < sel) sel = available;
+    if (sel > 2147483647LL) return -1;
+    return (int)sel;
+}
+
+int make_geom(long long n, int m, long long eb, long long ee, Geom* g) {
+    const int mk = macro_length(m, n);
+    if (mk < 0) return fail(FSMELD_E_SHORT, "Target is too short for this query length.");
+    g->n = n;
+    g->m = m;
+    g->m_k = mk;
+    g->kml = mk - m + 1;
+    g->tsn = n - m + 1;
+    g->forsize = g->tsn / g->kml;
+    const long long tail = g->tsn % g->kml;
+    g->tail_lo = (int)(g->kml - tail);
+    g->S = g->forsize + (tail > 0 ? 1 : 0);
+    g->excl_b = (eb >= 0 && ee > eb) ? eb : -1;
+    g->excl_e = (eb >= 0 && ee > eb) ? ee : -1;
+    return FSMELD_OK;
+}
+
+// ----------------------------------------------------------------- queries
+
+static int metric_p(int metric) { return (metric == DTW || metric == ERP) ? 2 : (metric == MSM ? 1 : 0); }
+
+// src/find_t_lp.cpp:148-186
+static double fn_D(double q, double C, int metric) {
+    if (metric == MSM) return C;
+    if (metric == ERP || metric == DTW) return (q - C) * (q - C);
+    return 1;
+}
+static double fn_tu(double q, double C, int metric) {
+    if (metric == MSM) return q - C;
+    if (metric == ERP) return q - std::fabs(q - C);
+    if (metric == EDR || metric == LCSS) return q - C;
+    return q;
+}
+static double fn_tl(double q, double C, int metric) {
+    if (metric == MSM) return q + C;
+    if (metric == ERP) return q + std::fabs(q - C);
+    if (metric == EDR || metric == LCSS) return q + C;
+    return q;
+}
+
+int prepare_query(const double* q, int m, int metric, int w, double arg, HostQuery* hq) {
+    if (m < 2) return fail(FSMELD_E_ARG, "m must be at least 2.");
+    if (w < 0 || w >= m) return fail(FSMELD_E_ARG, "w must satisfy 0 <= w < m.");
+    if (metric < DTW || metric > MSM) return fail(FSMELD_E_ARG, "Unsupported metric.");
+    if ((metric == EDR || metric == LCSS || metric == MSM) && !(arg >= 0))
+        return fail(FSMELD_E_ARG, "Matching tolerance and MSM cost must be non-negative.");
+    if (!std::isfinite(arg)) return fail(FSMELD_E_ARG, "Invalid finite metric parameter.");
+    double ex = 0, ex2 = 0;
+    for (int i = 0; i < m; ++i) {
+        if (!std::isfinite(q[i])) return fail(FSMELD_E_ARG, "Query must begin with m finite numeric values.");
+        ex += q[i];
+        ex2 += q[i] * q[i];
+    }
+    const double mean = ex / m;
+    double sd = ex2 / m;
+    sd = std::sqrt(sd - mean * mean);
+    if (!std::isfinite(sd) || sd <= 1e-12)
+        return fail(FSMELD_E_ARG,
+                    "Query cannot be z-normalized: non-finite or near-zero standard deviation.");
+    hq->m = m; hq->w = w; hq->metric = metric; hq->arg = arg; hq->p = metric_p(metric);
+    hq->qn.resize(m);
+    for (int i = 0; i < m; ++i) hq->qn[i] = (q[i] - mean) / sd;
+    const std::vector<double>& qn = hq->qn;
+    // query envelope (src/fsmeld.cpp:721): window extremes, most recent on ties
+    hq->LQ.resize(m); hq->UQ.resize(m);
+    for (int o = 0; o < m; ++o) {
+        const int a = std::max(0, o - w), b = std::min(m - 1, o + w);
+        double lo = qn[a], hi = qn[a];
+        for (int i = a + 1; i <= b; ++i) {
+            lo = (qn[i] <= lo) ? qn[i] : lo;
+            hi = (qn[i] >= hi) ? qn[i] : hi;
+        }
+        hq->LQ[o] = lo; hq->UQ[o] = hi;
+    }
+    hq->qs = qn;
+    std::sort(hq->qs.begin(), hq->qs.end());
+    hq->pw.resize(3 * m); hq->opw.resize(3 * m);
+    hq->Dq.resize(m); hq->tlq.resize(m); hq->tuq.resize(m);
+    hq->oD.resize(m); hq->otl.resize(m); hq->otu.resize(m);
+    for (int j = 0; j < m; ++j) {
+        for (int a = 0; a < 3; ++a) {
+            hq->pw[a * m + j] = std::pow(hq->qs[j], a);
+            hq->opw[a * m + j] = std::pow(qn[j], a);
+        }
+        hq->Dq[j] = fn_D(hq->qs[j], arg, metric);
+        hq->tlq[j] = fn_tl(hq->qs[j], arg, metric);
+        hq->tuq[j] = fn_tu(hq->qs[j], arg, metric);
+        hq->oD[j] = fn_D(qn[j], arg, metric);
+        hq->otl[j] = fn_tl(qn[j], arg, metric);
+        hq->otu[j] = fn_tu(qn[j], arg, metric);
+    }
+    auto order = [&](const std::vector<double>& key, bool desc) {
+        std::vector<int> o(m);
+        for (int i = 0; i < m; ++i) o[i] = i;
+        std::stable_sort(o.begin(), o.end(), [&](int a, int b) {
+            return desc ? key[a] > key[b] : key[a] < key[b];
+        });
+        return o;
+    };
+    hq->ordA_l = order(hq->otl, true);
+    hq->ordB_l = order(qn, true);
+    hq->ordA_u = order(hq->otu, false);
+    hq->ordB_u = order(qn, false);
+    return FSMELD_OK;
+}
+
+}  // namespace fsm
+
+// ------------------------------------------------------------------ context
+
+using namespace fsm;
+
+struct fsmeld_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double* d_target = nullptr;
+    long long n = 0;
+    bool own_target = false;
+    int sm_count = 148;
+    int smem_optin = 227 * 1024;
+    long long ws_limit = 0;
+    long long launches = 0;
+    std::string err;
+    struct Buf { void* p = nullptr; size_t bytes = 0; };
+    std::map<std::string, Buf> bufs;
+    std::map<int, double2*> twiddles;
+    std::map<const void*, int> smem_set;
+};
+
+namespace fsm {
+
+static size_t ws_total(const fsmeld_ctx* c) {
+    size_t t = 0;
+    for (auto& kv : c->bufs) t += kv.second.bytes;
+    return t;
+}
+
+static int buf(fsmeld_ctx* c, const std::string& name, size_t bytes, void** out) {
+    if (bytes == 0) bytes = 16;
+    auto& b = c->bufs[name];
+    if (b.bytes < bytes) {
+        if (b.p) { cudaFree(b.p); b.p = nullptr; b.bytes = 0; }
+        const size_t want = bytes + bytes / 8;
+        if (c->ws_limit > 0 && (long long)(ws_total(c) + want) > c->ws_limit)
+            return fail(FSMELD_E_NOMEM, "Device workspace budget exceeded.");
+        cudaError_t e = cudaMalloc(&b.p, want);
+        if (e != cudaSuccess) { b.p = nullptr; return cuda_fail(e, "cudaMalloc", __FILE__, __LINE__); }
+        b.bytes = want;
+    }
+    *out = b.p;
+    return FSMELD_OK;
+}
+
+template <typename T>
+static int bufT(fsmeld_ctx* c, const std::string& name, size_t count, T** out) {
+    void* p;
+    int r = buf(c, name, count * sizeof(T), &p);
+    *out = (T*)p;
+    return r;
+}
+
+template <typename K>
+static int allow_smem(fsmeld_ctx* c, K kernel, size_t bytes) {
+    if (bytes > (size_t)c->smem_optin) return fail(FSMELD_E_UNSUPPORTED, "shared memory request too large");
+    int& cur = c->smem_set[(const void*)kernel];
+    if ((size_t)cur < bytes) {
+        FSM_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        cur = (int)bytes;
+    }
+    return FSMELD_OK;
+}
+
+#define LAUNCH_CHECK(c)                                                  \
+    do {                                                                 \
+        (c)->launches++;                                                 \
+        cudaError_t _le = cudaGetLastError();                            \
+        if (_le != cudaSuccess) return cuda_fail(_le, "kernel launch", __FILE__, __LINE__); \
+    } while (0)
+
+static int twiddle_table(fsmeld_ctx* c, int P, const double2** out) {
+    auto it = c->twiddles.find(P);
+    if (it != c->twiddles.end()) { *out = it->second; return FSMELD_OK; }
+    std::vector<double2> w(P);
+    for (int k = 0; k < P; ++k) {
+        const double ang = 6.283185307179586476925286766559 * (double)k / (double)P;
+        w[k] = make_double2(std::cos(ang), -std::sin(ang));
+    }
+    double2* d;
+    FSM_CUDA_TRY(cudaMalloc(&d, sizeof(double2) * P));
+    FSM_CUDA_TRY(cudaMemcpy(d, w.data(), sizeof(double2) * P, cudaMemcpyHostToDevice));
+    c->twiddles[P] = d;
+    *out = d;
+    return FSMELD_OK;
+}
+
+// upload a prepared query into a named device slot
+static int upload_query(fsmeld_ctx* c, const HostQuery& hq, const std::string& slot, QueryDev* qd) {
+    const int m = hq.m;
+    const size_t nd = (size_t)m * (3 + 4 + 3 + 3 + 3 + 3), ni = (size_t)m * 4;
+    std::vector<unsigned char> host(nd * 8 + ni * 4);
+    double* d = (double*)host.data();
+    size_t o = 0;
+    auto put = [&](const std::vector<double>& v) { memcpy(d + o, v.data(), v.size() * 8); size_t at = o; o += v.size(); return at; };
+    const size_t o_qn = put(hq.qn), o_LQ = put(hq.LQ), o_UQ = put(hq.UQ), o_qs = put(hq.qs);
+    const size_t o_pw = put(hq.pw), o_Dq = put(hq.Dq), o_tlq = put(hq.tlq), o_tuq = put(hq.tuq);
+    const size_t o_opw = put(hq.opw), o_oD = put(hq.oD), o_otl = put(hq.otl), o_otu = put(hq.otu);
+    int* ip = (int*)(d + nd);
+    memcpy(ip, hq.ordA_l.data(), m * 4);
+    memcpy(ip + m, hq.ordB_l.data(), m * 4);
+    memcpy(ip + 2 * m, hq.ordA_u.data(), m * 4);
+    memcpy(ip + 3 * m, hq.ordB_u.data(), m * 4);
+    void* dev;
+    int r = buf(c, slot, host.size(), &dev);
+    if (r) return r;
+    FSM_CUDA_TRY(cudaMemcpyAsync(dev, host.data(), host.size(), cudaMemcpyHostToDevice, c->stream));
+    FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));  // host staging buffer is released on return
+    const double* D = (const double*)dev;
+    const int* I = (const int*)(D + nd);
+    qd->m = m; qd->w = hq.w; qd->metric = hq.metric; qd->p = hq.p; qd->arg = hq.arg;
+    qd->cutoff = 0.0;
+    qd->qn = D + o_qn; qd->LQ = D + o_LQ; qd->UQ = D + o_UQ; qd->qs = D + o_qs;
+    qd->pw = D + o_pw; qd->Dq = D + o_Dq; qd->tlq = D + o_tlq; qd->tuq = D + o_tuq;
+    qd->opw = D + o_opw; qd->oD = D + o_oD; qd->otl = D + o_otl; qd->otu = D + o_otu;
+    qd->ordA_l = I; qd->ordB_l = I + m; qd->ordA_u = I + 2 * m; qd->ordB_u = I + 3 * m;
+    return FSMELD_OK;
+}
+
+// ------------------------------------------------------------- pipeline
+
+struct Stats {
+    double* MU = nullptr;
+    double* SIG = nullptr;
+    double* Un = nullptr;
+    double* Ln = nullptr;
+};
+
+static int run_stats(fsmeld_ctx* c, const Geom& g, Stats* st, const std::string& tag) {
+    int r;
+    if ((r = bufT(c, "mu" + tag, (size_t)g.S * g.kml, &st->MU))) return r;
+    if ((r = bufT(c, "sig" + tag, (size_t)g.S * g.kml, &st->SIG))) return r;
+    const size_t smem = mvmean_smem_bytes();
+    if ((r = allow_smem(c, k_mvmean, smem))) return r;
+    const unsigned blocks = (unsigned)((g.S + 31) / 32);
+    k_mvmean<<<blocks, 32, smem, c->stream>>>(c->d_target, g, st->MU, st->SIG);
+    LAUNCH_CHECK(c);
+    return FSMELD_OK;
+}
+
+template <int T, int OPT>
+static int launch_env(fsmeld_ctx* c, const Geom& g, int w, Stats* st) {
+    const size_t work = envelope_work_bytes(g.m_k);
+    double* gwork = nullptr;
+    size_t smem = work;
+    unsigned grid;
+    int r;
+    if (work + 8192 <= (size_t)c->smem_optin) {
+        if ((r = allow_smem(c, k_envelope<T, OPT>, smem))) return r;
+        int per_sm = 0;
+        FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_envelope<T, OPT>, T, smem));
+        grid = (unsigned)std::min<long long>(g.S, (long long)std::max(1, per_sm) * c->sm_count);
+    } else {
+        smem = 0;
+        grid = (unsigned)std::min<long long>(g.S, (long long)c->sm_count * 2);
+        if ((r = bufT(c, "envwork", (work / 8 + 1) * grid, &gwork))) return r;
+    }
+    k_envelope<T, OPT><<<grid, T, smem, c->stream>>>(c->d_target, st->MU, st->SIG, g, w, st->Un, st->Ln,
+                                                     gwork, (long long)(work / 8 + 1));
+    LAUNCH_CHECK(c);
+    return FSMELD_OK;
+}
+
+static int run_env(fsmeld_ctx* c, const Geom& g, int w, Stats* st, const std::string& tag) {
+    int r;
+    if ((r = bufT(c, "un" + tag, (size_t)g.S * g.m_k, &st->Un))) return r;
+    if ((r = bufT(c, "ln" + tag, (size_t)g.S * g.m_k, &st->Ln))) return r;
+    const int mk = g.m_k;
+    if (mk <= 1024) return launch_env<128, 8>(c, g, w, st);
+    if (mk <= 2048) return launch_env<256, 8>(c, g, w, st);
+    if (mk <= 4096) return launch_env<512, 8>(c, g, w, st);
+    if (mk <= 8192) return launch_env<1024, 8>(c, g, w, st);
+    if (mk <= 16384) return launch_env<1024, 16>(c, g, w, st);
+    return fail(FSMELD_E_UNSUPPORTED, "macro segments longer than 16384 points are not supported");
+}
+
+template <int T, int IPT>
+static int launch_thr(fsmeld_ctx* c, const Geom& g, const ThrJob* djobs, int njobs, int m) {
+    const size_t work = threshold_work_bytes(T * IPT, threshold_sort_tmp_bytes<T, IPT>(), m);
+    unsigned char* gwork = nullptr;
+    size_t smem = work;
+    unsigned gx;
+    int r;
+    if (work + 16384 <= (size_t)c->smem_optin) {
+        if ((r = allow_smem(c, k_threshold<T, IPT>, smem))) return r;
+        int per_sm = 0;
+        FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_threshold<T, IPT>, T, smem));
+        gx = (unsigned)std::min<long long>(2 * g.S, (long long)std::max(1, per_sm) * c->sm_count * 4);
+    } else {
+        smem = 0;
+        gx = (unsigned)std::min<long long>(2 * g.S, (long long)c->sm_count * 2);
+        if ((r = bufT(c, "thrwork", work * gx * (size_t)njobs, &gwork))) return r;
+    }
+    dim3 grid(gx, njobs);
+    k_threshold<T, IPT><<<grid, T, smem, c->stream>>>(g, djobs, gwork, (long long)work);
+    LAUNCH_CHECK(c);
+    return FSMELD_OK;
+}
+
+static int run_thr(fsmeld_ctx* c, const Geom& g, const std::vector<ThrJob>& jobs) {
+    if (jobs.empty()) return FSMELD_OK;
+    ThrJob* dj;
+    int r;
+    if ((r = bufT(c, "thrjobs", jobs.size(), &dj))) return r;
+    FSM_CUDA_TRY(cudaMemcpyAsync(dj, jobs.data(), sizeof(ThrJob) * jobs.size(), cudaMemcpyHostToDevice, c->stream));
+    const int m = g.m;
+    const int cnt = g.m_k - 2 * m + 2;
+    const int nj = (int)jobs.size();
+    if (cnt <= 512) r = launch_thr<128, 4>(c, g, dj, nj, m);
+    else if (cnt <= 1024) r = launch_thr<256, 4>(c, g, dj, nj, m);
+    else if (cnt <= 2048) r = launch_thr<256, 8>(c, g, dj, nj, m);
+    else if (cnt <= 4096) r = launch_thr<512, 8>(c, g, dj, nj, m);
+    else if (cnt <= 8192) r = launch_thr<1024, 8>(c, g, dj, nj, m);
+    else if (cnt <= 16384) r = launch_thr<1024, 16>(c, g, dj, nj, m);
+    else r = fail(FSMELD_E_UNSUPPORTED, "envelope core longer than 16384 points is not supported");
+    if (r) return r;
+    // the job array is read by the kernel: keep it alive until it finishes
+    FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return FSMELD_OK;
+}
+
+static int run_lbip(fsmeld_ctx* c, const Geom& g, LbJob job) {
+    int P = 1, logP = 0;
+    while (P < g.m_k) { P <<= 1; ++logP; }
+    const double2* W;
+    int r;
+    if ((r = twiddle_table(c, P, &W))) return r;
+    size_t smem = lbip_smem_bytes(P, g.m_k, g.m, job.q.metric);
+    unsigned grid;
+    if (smem + 8192 <= (size_t)c->smem_optin) {
+        job.gwork = nullptr;
+        if ((r = allow_smem(c, k_lbip<256>, smem))) return r;
+        int per_sm = 0;
+        FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lbip<256>, 256, smem));
+        grid = (unsigned)std::min<long long>(g.S, (long long)std::max(1, per_sm) * c->sm_count);
+    } else {
+        grid = (unsigned)std::min<long long>(g.S, (long long)c->sm_count * 2);
+        unsigned char* gw;
+        if ((r = bufT(c, "lbwork", smem * grid, &gw))) return r;
+        job.gwork = gw;
+        job.slot_stride = (long long)smem;
+        smem = 0;
+    }
+    k_lbip<256><<<grid, 256, smem, c->stream>>>(g, job, W, P, logP);
+    LAUNCH_CHECK(c);
+    return FSMELD_OK;
+}
+
+// counters slot layout
+enum { C_SURV, C_G1, C_G2, C_OUT, C_VALID, C_SEED, C_SEEDOUT, C_N };
+
+static int run_glb(fsmeld_ctx* c, const Geom& g, const QueryDev& qd, const Stats& st, const long long* in,
+                   unsigned long long* cnt, long long cap, long long* segc, long long** out_list) {
+    long long *g1, *g2;
+    double *g1b, *g1t;
+    int r;
+    if ((r = bufT(c, "g1", (size_t)cap, &g1))) return r;
+    if ((r = bufT(c, "g1b", (size_t)cap, &g1b))) return r;
+    if ((r = bufT(c, "g1t", (size_t)cap, &g1t))) return r;
+    if ((r = bufT(c, "g2", (size_t)cap, &g2))) return r;
+    GlbJob j1{};
+    j1.q = qd; j1.target = c->d_target; j1.MU = st.MU; j1.SIG = st.SIG;
+    j1.in = in; j1.n_in = cnt + C_SURV; j1.in_cap = cap;
+    j1.out = g1; j1.out_b = g1b; j1.out_t = g1t; j1.n_out = cnt + C_G1; j1.out_cap = cap;
+    j1.segc = segc;
+    const size_t sm1 = sizeof(double) * 3 * qd.m;
+    if ((r = allow_smem(c, k_glb_tq, sm1))) return r;
+    k_glb_tq<<<c->sm_count * 8, 256, sm1, c->stream>>>(g, j1);
+    LAUNCH_CHECK(c);
+    GlbJob j2 = j1;
+    j2.in = g1; j2.in_b = g1b; j2.in_t = g1t; j2.n_in = cnt + C_G1;
+    j2.out = g2; j2.out_b = nullptr; j2.out_t = nullptr; j2.n_out = cnt + C_G2;
+    int warps = 8;
+    while (warps > 1 && sizeof(double) * (size_t)qd.m * (1 + 2 * warps) > (size_t)c->smem_optin - 4096) warps >>= 1;
+    const size_t sm2 = sizeof(double) * (size_t)qd.m * (1 + 2 * warps);
+    if ((r = allow_smem(c, k_glb_qt, sm2))) return r;
+    k_glb_qt<<<c->sm_count * 4, warps * 32, sm2, c->stream>>>(g, j2);
+    LAUNCH_CHECK(c);
+    *out_list = g2;
+    return FSMELD_OK;
+}
+
+static int run_dp(fsmeld_ctx* c, const Geom& g, DpJob job, long long expected) {
+    const int w = job.q.w;
+    const int warps = 4;
+    const size_t per_warp = dp_warp_doubles(w);
+    size_t smem = sizeof(double) * (((size_t)job.q.m + 1) & ~(size_t)1) + sizeof(double) * per_warp * warps;
+    unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>((expected + warps * 32 - 1) / (warps * 32),
+                                                                        (long long)c->sm_count * 16));
+    int r;
+    job.gwork = nullptr;
+    if (smem > (size_t)c->smem_optin - 4096) {
+        grid = (unsigned)std::min<long long>(grid, (long long)c->sm_count * 4);
+        double* gw;
+        if ((r = bufT(c, "dpwork", per_warp * warps * grid, &gw))) return r;
+        job.gwork = gw;
+        smem = sizeof(double) * (((size_t)job.q.m + 1) & ~(size_t)1);
+    }
+    switch (job.q.metric) {
+        case DTW: if ((r = allow_smem(c, k_dp<DTW>, smem))) return r; k_dp<DTW><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
+        case ERP: if ((r = allow_smem(c, k_dp<ERP>, smem))) return r; k_dp<ERP><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
+        case EDR: if ((r = allow_smem(c, k_dp<EDR>, smem))) return r; k_dp<EDR><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
+        case LCSS: if ((r = allow_smem(c, k_dp<LCSS>, smem))) return r; k_dp<LCSS><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
+        default: if ((r = allow_smem(c, k_dp<MSM>, smem))) return r; k_dp<MSM><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
+    }
+    LAUNCH_CHECK(c);
+    return FSMELD_OK;
+}
+
+// sort int64 keys (optionally with double values) in place through a scratch copy
+static int sort_pairs_i64(fsmeld_ctx* c, long long* keys, double* vals, long long n) {
+    if (n <= 1) return FSMELD_OK;
+    long long* k2;
+    double* v2 = nullptr;
+    int r;
+    if ((r = bufT(c, "sortk", (size_t)n, &k2))) return r;
+    if (vals && (r = bufT(c, "sortv", (size_t)n, &v2))) return r;
+    size_t tmp = 0;
+    if (vals) FSM_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys, k2, vals, v2, (int)n, 0, 64, c->stream));
+    else FSM_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tmp, keys, k2, (int)n, 0, 64, c->stream));
+    void* t;
+    if ((r = buf(c, "sorttmp", tmp, &t))) return r;
+    if (vals) FSM_CUDA_TRY(cub::DeviceRadixSort::SortPairs(t, tmp, keys, k2, vals, v2, (int)n, 0, 64, c->stream));
+    else FSM_CUDA_TRY(cub::DeviceRadixSort::SortKeys(t, tmp, keys, k2, (int)n, 0, 64, c->stream));
+    FSM_CUDA_TRY(cudaMemcpyAsync(keys, k2, sizeof(long long) * n, cudaMemcpyDeviceToDevice, c->stream));
+    if (vals) FSM_CUDA_TRY(cudaMemcpyAsync(vals, v2, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    return FSMELD_OK;
+}
+
+// lexicographic (distance, index) order: index sort, then stable distance sort
+static int sort_lex(fsmeld_ctx* c, long long* idx, double* dist, long long n) {
+    int r;
+    if ((r = sort_pairs_i64(c, idx, dist, n))) return r;
+    if (n <= 1) return FSMELD_OK;
+    long long* k2;
+    double* d2;
+    if ((r = bufT(c, "sortk", (size_t)n, &k2))) return r;
+    if ((r = bufT(c, "sortv", (size_t)n, &d2))) return r;
+    size_t tmp = 0;
+    FSM_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp, dist, d2, idx, k2, (int)n, 0, 64, c->stream));
+    void* t;
+    if ((r = buf(c, "sorttmp", tmp, &t))) return r;
+    FSM_CUDA_TRY(cub::DeviceRadixSort::SortPairs(t, tmp, dist, d2, idx, k2, (int)n, 0, 64, c->stream));
+    FSM_CUDA_TRY(cudaMemcpyAsync(idx, k2, sizeof(long long) * n, cudaMemcpyDeviceToDevice, c->stream));
+    FSM_CUDA_TRY(cudaMemcpyAsync(dist, d2, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    return FSMELD_OK;
+}
+
+struct QueryRun {
+    const HostQuery* hq;
+    int mode;  // 0 search, 1 cutoff, 2 exact
+    double cutoff;
+    int k;
+    long long eb, ee;
+    int64_t* out_idx;
+    double* out_dist;
+    int64_t cap;
+    int64_t* out_count;
+    fsmeld_counters* cnt;
+    int64_t* seg_counts;
+};
+
+static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& st, bool have_env) {
+    int r;
+    Geom g = g0;
+    g.excl_b = (qr.eb >= 0 && qr.ee > qr.eb) ? qr.eb : -1;
+    g.excl_e = (qr.eb >= 0 && qr.ee > qr.eb) ? qr.ee : -1;
+    const HostQuery& hq = *qr.hq;
+    QueryDev qd;
+    if ((r = upload_query(c, hq, "query", &qd))) return r;
+    unsigned long long* cnt;
+    if ((r = bufT(c, "counters", C_N, &cnt))) return r;
+    FSM_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, c->stream));
+    const long long cap = g.tsn;
+    unsigned long long h[C_N] = {0};
+    fsmeld_counters out{};
+    out.m_k = g.m_k;
+    out.segments = g.forsize;
+    out.tail = g.tsn % g.kml;
+
+    if (qr.mode == 2) {  // exact: every valid window through the DP
+        long long *oi;
+        double* od;
+        if ((r = bufT(c, "outi", (size_t)cap, &oi))) return r;
+        if ((r = bufT(c, "outd", (size_t)cap, &od))) return r;
+        qd.cutoff = qr.cutoff;
+        DpJob dj{};
+        dj.q = qd; dj.target = c->d_target; dj.MU = st.MU; dj.SIG = st.SIG;
+        dj.list = nullptr; dj.n_windows = g.tsn; dj.mode = 0; dj.cutoff = qr.cutoff;
+        dj.out_idx = oi; dj.out_dist = od; dj.n_out = cnt + C_OUT; dj.out_cap = cap; dj.n_valid = cnt + C_VALID;
+        if ((r = run_dp(c, g, dj, g.tsn))) return r;
+        FSM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+        FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        const long long nout = (long long)h[C_OUT];
+        if ((r = sort_pairs_i64(c, oi, od, nout))) return r;
+        const long long ncopy = std::min<long long>(nout, qr.cap);
+        if (ncopy > 0) {
+            FSM_CUDA_TRY(cudaMemcpyAsync(qr.out_idx, oi, sizeof(long long) * ncopy, cudaMemcpyDeviceToHost, c->stream));
+            if (qr.out_dist) FSM_CUDA_TRY(cudaMemcpyAsync(qr.out_dist, od, sizeof(double) * ncopy, cudaMemcpyDeviceToHost, c->stream));
+        }
+        FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        out.valid = (long long)h[C_VALID];
+        out.invalid = g.tsn - out.valid;
+        out.after_lb = out.after_glb = out.exact_evals = out.valid;
+        out.matches = nout;
+        out.threshold = qr.cutoff;
+        if (qr.out_count) *qr.out_count = nout;
+        if (qr.cnt) *qr.cnt = out;
+        return FSMELD_OK;
+    }
+
+    // thresholds
+    double* thr;
+    if ((r = bufT(c, "thr", (size_t)2 * g.S, &thr))) return r;
+    std::vector<ThrJob> jobs(1);
+    jobs[0].q = qd; jobs[0].Un = st.Un; jobs[0].Ln = st.Ln; jobs[0].thr = thr;
+    if ((r = run_thr(c, g, jobs))) return r;
+    (void)have_env;
+
+    long long* segc = nullptr;
+    if ((r = bufT(c, "segc", (size_t)3 * g.S, &segc))) return r;
+
+    if (qr.mode == 0) {  // search
+        long long* surv;
+        if ((r = bufT(c, "surv", (size_t)cap, &surv))) return r;
+        qd.cutoff = qr.cutoff;
+        LbJob lj{};
+        lj.q = qd; lj.Un = st.Un; lj.Ln = st.Ln; lj.thr = thr; lj.SIG = st.SIG;
+        lj.zout = nullptr; lj.surv = surv; lj.surv_cap = cap; lj.nsurv = cnt + C_SURV;
+        lj.nvalid = cnt + C_VALID; lj.segc = segc;
+        if ((r = run_lbip(c, g, lj))) return r;
+        long long* g2;
+        if ((r = run_glb(c, g, qd, st, surv, cnt, cap, segc, &g2))) return r;
+        long long* oi;
+        double* od;
+        if ((r = bufT(c, "outi", (size_t)cap, &oi))) return r;
+        if ((r = bufT(c, "outd", (size_t)cap, &od))) return r;
+        DpJob dj{};
+        dj.q = qd; dj.target = c->d_target; dj.MU = st.MU; dj.SIG = st.SIG;
+        dj.list = g2; dj.n_list = cnt + C_G2; dj.list_cap = cap; dj.mode = 0; dj.cutoff = qr.cutoff;
+        dj.out_idx = oi; dj.out_dist = od; dj.n_out = cnt + C_OUT; dj.out_cap = cap; dj.n_valid = nullptr;
+        if ((r = run_dp(c, g, dj, (long long)c->sm_count * 16 * 128))) return r;
+        FSM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+        FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        const long long nout = (long long)h[C_OUT];
+        if ((r = sort_pairs_i64(c, oi, nullptr, nout))) return r;
+        const long long ncopy = std::min<long long>(nout, qr.cap);
+        if (ncopy > 0)
+            FSM_CUDA_TRY(cudaMemcpyAsync(qr.out_idx, oi, sizeof(long long) * ncopy, cudaMemcpyDeviceToHost, c->stream));
+        if (qr.seg_counts && g.forsize > 0)
+            FSM_CUDA_TRY(cudaMemcpyAsync(qr.seg_counts, segc, sizeof(long long) * 3 * g.forsize,
+                                         cudaMemcpyDeviceToHost, c->stream));
+        FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        out.valid = (long long)h[C_VALID];
+        out.invalid = g.tsn - out.valid;
+        out.after_lb = (long long)h[C_SURV];
+        out.after_glb = (long long)h[C_G2];
+        out.exact_evals = out.after_glb;
+        out.matches = nout;
+        out.threshold = qr.cutoff;
+        if (qr.out_count) *qr.out_count = nout;
+        if (qr.cnt) *qr.cnt = out;
+        return FSMELD_OK;
+    }
+
+    // cutoff (top-k)
+    double* z;
+    if ((r = bufT(c, "zbuf", (size_t)g.S * g.kml, &z))) return r;
+    LbJob lj{};
+    lj.q = qd; lj.Un = st.Un; lj.Ln = st.Ln; lj.thr = thr; lj.SIG = st.SIG;
+    lj.zout = z; lj.surv = nullptr; lj.nsurv = cnt + C_SURV; lj.nvalid = cnt + C_VALID; lj.segc = nullptr;
+    if ((r = run_lbip(c, g, lj))) return r;
+    // seeds
+    long long* seeds;
+    if ((r = bufT(c, "seeds", (size_t)g.S, &seeds))) return r;
+    k_seed<<<(unsigned)std::min<long long>(g.S, (long long)c->sm_count * 8), 256, 0, c->stream>>>(
+        g, z, st.SIG, 1, seeds, cnt + C_SEED, g.S);
+    LAUNCH_CHECK(c);
+    long long* si;
+    double* sd;
+    if ((r = bufT(c, "seedi", (size_t)g.S, &si))) return r;
+    if ((r = bufT(c, "seedd", (size_t)g.S, &sd))) return r;
+    DpJob sj{};
+    sj.q = qd; sj.target = c->d_target; sj.MU = st.MU; sj.SIG = st.SIG;
+    sj.list = seeds; sj.n_list = cnt + C_SEED; sj.list_cap = g.S; sj.mode = 1; sj.cutoff = 0.0;
+    sj.out_idx = si; sj.out_dist = sd; sj.n_out = cnt + C_SEEDOUT; sj.out_cap = g.S;
+    if ((r = run_dp(c, g, sj, g.S))) return r;
+    FSM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const long long nvalid = (long long)h[C_VALID];
+    if (nvalid < qr.k) return fail(FSMELD_E_FEWER_K, "Fewer valid, non-excluded candidates than requested k.");
+    double tau = DBL_MAX;
+    const long long nseed = (long long)h[C_SEEDOUT];
+    if (nseed >= qr.k) {
+        std::vector<double> hd(nseed);
+        FSM_CUDA_TRY(cudaMemcpy(hd.data(), sd, sizeof(double) * nseed, cudaMemcpyDeviceToHost));
+        std::nth_element(hd.begin(), hd.begin() + (qr.k - 1), hd.end());
+        tau = hd[qr.k - 1];
+    }
+    // filter, GLB and DP at tau
+    long long* f1;
+    if ((r = bufT(c, "surv", (size_t)cap, &f1))) return r;
+    k_lb_filter<<<(unsigned)std::min<long long>((g.tsn + 255) / 256, (long long)c->sm_count * 16), 256, 0, c->stream>>>(
+        g, z, st.SIG, tau, qd.metric, f1, cnt + C_SURV, cap);
+    LAUNCH_CHECK(c);
+    QueryDev qt = qd;
+    qt.cutoff = tau;
+    long long* g2;
+    if ((r = run_glb(c, g, qt, st, f1, cnt, cap, nullptr, &g2))) return r;
+    long long* oi;
+    double* od;
+    if ((r = bufT(c, "outi", (size_t)cap, &oi))) return r;
+    if ((r = bufT(c, "outd", (size_t)cap, &od))) return r;
+    DpJob dj{};
+    dj.q = qt; dj.target = c->d_target; dj.MU = st.MU; dj.SIG = st.SIG;
+    dj.list = g2; dj.n_list = cnt + C_G2; dj.list_cap = cap; dj.mode = 1; dj.cutoff = tau;
+    dj.out_idx = oi; dj.out_dist = od; dj.n_out = cnt + C_OUT; dj.out_cap = cap;
+    if ((r = run_dp(c, g, dj, (long long)c->sm_count * 16 * 128))) return r;
+    FSM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const long long nout = (long long)h[C_OUT];
+    if (nout < qr.k) return fail(FSMELD_E_FEWER_K, "Fewer valid, non-excluded candidates than requested k.");
+    if ((r = sort_lex(c, oi, od, nout))) return r;
+    FSM_CUDA_TRY(cudaMemcpyAsync(qr.out_idx, oi, sizeof(long long) * qr.k, cudaMemcpyDeviceToHost, c->stream));
+    std::vector<double> kd(qr.k);
+    FSM_CUDA_TRY(cudaMemcpyAsync(kd.data(), od, sizeof(double) * qr.k, cudaMemcpyDeviceToHost, c->stream));
+    FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (qr.out_dist) memcpy(qr.out_dist, kd.data(), sizeof(double) * qr.k);
+    out.valid = nvalid;
+    out.invalid = g.tsn - nvalid;
+    out.after_lb = (long long)h[C_SURV];
+    out.after_glb = (long long)h[C_G2];
+    out.exact_evals = (long long)h[C_G2] + nseed;
+    out.matches = qr.k;
+    out.threshold = kd[qr.k - 1];
+    if (qr.out_count) *qr.out_count = qr.k;
+    if (qr.cnt) *qr.cnt = out;
+    return FSMELD_OK;
+}
+
+// One call over many queries: statistics per distinct m, envelopes per distinct (m, w).
+int run_batch(fsmeld_ctx* c, std::vector<QueryRun>& runs, std::vector<int>* status) {
+    status->assign(runs.size(), FSMELD_OK);
+    std::vector<size_t> order(runs.size());
+    for (size_t i = 0; i < runs.size(); ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+        if (runs[a].hq->m != runs[b].hq->m) return runs[a].hq->m < runs[b].hq->m;
+        return runs[a].hq->w < runs[b].hq->w;
+    });
+    int cur_m = -1, cur_w = -1;
+    Stats st;
+    Geom g{};
+    bool have_env = false;
+    int first_err = FSMELD_OK;
+    for (size_t oi = 0; oi < order.size(); ++oi) {
+        QueryRun& qr = runs[order[oi]];
+        const int m = qr.hq->m, w = qr.hq->w;
+        int r = FSMELD_OK;
+        if (m != cur_m) {
+            have_env = false;
+            cur_w = -1;
+            r = make_geom(c->n, m, -1, -1, &g);
+            if (!r) r = run_stats(c, g, &st, "");
+            cur_m = r ? -1 : m;
+        }
+        if (!r && qr.mode != 2 && w != cur_w) {
+            r = run_env(c, g, w, &st, "");
+            cur_w = r ? -1 : w;
+            have_env = !r;
+        }
+        if (!r) r = run_query(c, qr, g, st, have_env);
+        (*status)[order[oi]] = r;
+        if (r && !first_err) first_err = r;
+        if (r == FSMELD_E_CUDA) break;
+    }
+    return first_err;
+}
+
+}  // namespace fsm
+
+// ====================================================================== C ABI
+
+extern "C" {
+
+static int open_common(int device, fsmeld_ctx** out) {
+    fsmeld_ctx* c = new fsmeld_ctx();
+    c->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaSetDevice", __FILE__, __LINE__); }
+    cudaDeviceProp prop;
+    e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaGetDeviceProperties", __FILE__, __LINE__); }
+    c->sm_count = prop.multiProcessorCount;
+    c->smem_optin = (int)prop.sharedMemPerBlockOptin;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        delete c;
+        return fail(FSMELD_E_CUDA, "stream/event creation failed");
+    }
+    static std::once_flag w16;
+    static int w16_status = 0;
+    std::call_once(w16, [] { w16_status = lbip_set_w16(); });
+    if (w16_status) { delete c; return w16_status; }
+    *out = c;
+    return FSMELD_OK;
+}
+
+int fsmeld_open(int device, const double* host_target, int64_t n, fsmeld_ctx** out) {
+    if (!out || !host_target || n <= 0) return fail(FSMELD_E_ARG, "invalid target");
+    fsmeld_ctx* c;
+    int r = open_common(device, &c);
+    if (r) return r;
+    cudaError_t e = cudaMalloc(&c->d_target, sizeof(double) * n);
+    if (e != cudaSuccess) { fsmeld_close(c); return cuda_fail(e, "cudaMalloc(target)", __FILE__, __LINE__); }
+    e = cudaMemcpy(c->d_target, host_target, sizeof(double) * n, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { fsmeld_close(c); return cuda_fail(e, "cudaMemcpy(target)", __FILE__, __LINE__); }
+    c->n = n;
+    c->own_target = true;
+    *out = c;
+    return FSMELD_OK;
+}
+
+int fsmeld_open_device(int device, const double* device_target, int64_t n, fsmeld_ctx** out) {
+    if (!out || !device_target || n <= 0) return fail(FSMELD_E_ARG, "invalid target");
+    fsmeld_ctx* c;
+    int r = open_common(device, &c);
+    if (r) return r;
+    c->d_target = const_cast<double*>(device_target);
+    c->n = n;
+    c->own_target = false;
+    *out = c;
+    return FSMELD_OK;
+}
+
+int fsmeld_open_file(int device, const char* path, fsmeld_ctx** out) {
+    FILE* f = path ? fopen(path, "rb") : nullptr;
+    if (!f) return fail(FSMELD_E_IO, "Cannot open target file.");
+    fseek(f, 0, SEEK_END);
+    const long long bytes = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    if (bytes <= 0 || bytes % 8) { fclose(f); return fail(FSMELD_E_IO, "Target file size is not a multiple of 8 bytes."); }
+    std::vector<double> t(bytes / 8);
+    const size_t got = fread(t.data(), 8, t.size(), f);
+    fclose(f);
+    if (got != t.size()) return fail(FSMELD_E_IO, "Short read of target file.");
+    return fsmeld_open(device, t.data(), (int64_t)t.size(), out);
+}
+
+int fsmeld_close(fsmeld_ctx* c) {
+    if (!c) return FSMELD_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto& kv : c->bufs) if (kv.second.p) cudaFree(kv.second.p);
+    for (auto& kv : c->twiddles) cudaFree(kv.second);
+    if (c->own_target && c->d_target) cudaFree(c->d_target);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return FSMELD_OK;
+}
+
+int64_t fsmeld_target_length(const fsmeld_ctx* c) { return c ? c->n : 0; }
+
+const char* fsmeld_last_error(const fsmeld_ctx* c) {
+    (void)c;
+    return g_last_error.c_str();
+}
+
+const char* fsmeld_strerror(int s) {
+    switch (s) {
+        case FSMELD_OK: return "ok";
+        case FSMELD_E_ARG: return "invalid argument";
+        case FSMELD_E_CUDA: return "CUDA error";
+        case FSMELD_E_NOMEM: return "out of device memory or workspace budget";
+        case FSMELD_E_SHORT: return "target shorter than 2*m-1 points";
+        case FSMELD_E_FEWER_K: return "fewer valid candidates than k";
+        case FSMELD_E_UNSUPPORTED: return "unsupported configuration";
+        case FSMELD_E_IO: return "I/O error";
+        default: return "unknown error";
+    }
+}
+
+int fsmeld_set_workspace_limit(fsmeld_ctx* c, int64_t bytes) {
+    if (!c) return FSMELD_E_ARG;
+    c->ws_limit = bytes;
+    return FSMELD_OK;
+}
+
+int64_t fsmeld_kernel_launches(const fsmeld_ctx* c) { return c ? c->launches : 0; }
+
+static int single(fsmeld_ctx* c, int mode, const double* query, int m, double cutoff, int k, int metric,
+                  int w, double arg, int64_t eb, int64_t ee, int64_t* out_idx, double* out_dist,
+                  int64_t cap, int64_t* out_count, fsmeld_counters* counters, int64_t* seg_counts) {
+    if (!c || !query) return fail(FSMELD_E_ARG, "null context or query");
+    if (mode != 1 && !(std::isfinite(cutoff) && cutoff >= 0))
+        return fail(FSMELD_E_ARG, "cutoff must be finite and non-negative.");
+    if (mode == 1 && (k < 1 || (long long)k > c->n - m + 1))
+        return fail(FSMELD_E_ARG, "k exceeds the candidate count or supported integer range.");
+    if (eb >= 0 || ee >= 0) {
+        if (eb < 0 || ee <= eb) return fail(FSMELD_E_ARG, "Exclusion requires 0 <= start < end.");
+    }
+    FSM_CUDA_TRY(cudaSetDevice(c->device));
+    HostQuery hq;
+    int r = prepare_query(query, m, metric, w, arg, &hq);
+    if (r) return r;
+    QueryRun qr{&hq, mode, cutoff, k, eb, ee, out_idx, out_dist, cap, out_count, counters, seg_counts};
+    std::vector<QueryRun> runs{qr};
+    std::vector<int> st;
+    cudaEventRecord(c->ev0, c->stream);
+    r = run_batch(c, runs, &st);
+    cudaEventRecord(c->ev1, c->stream);
+    cudaEventSynchronize(c->ev1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    if (counters) counters->device_ms = ms;
+    return r;
+}
+
+int fsmeld_search(fsmeld_ctx* c, const double* query, int m, double cutoff, int metric, int w, double arg,
+                  int64_t eb, int64_t ee, int64_t* out_idx, int64_t cap, int64_t* out_count,
+                  fsmeld_counters* counters, int64_t* seg_counts) {
+    return single(c, 0, query, m, cutoff, 0, metric, w, arg, eb, ee, out_idx, nullptr, cap, out_count,
+                  counters, seg_counts);
+}
+
+int fsmeld_cutoff(fsmeld_ctx* c, const double* query, int m, int k, int metric, int w, double arg,
+                  int64_t eb, int64_t ee, int64_t* out_idx, double* out_dist, fsmeld_counters* counters) {
+    int64_t cnt = 0;
+    return single(c, 1, query, m, 0.0, k, metric, w, arg, eb, ee, out_idx, out_dist, k, &cnt, counters,
+                  nullptr);
+}
+
+int fsmeld_exact(fsmeld_ctx* c, const double* query, int m, double cutoff, int metric, int w, double arg,
+                 int64_t eb, int64_t ee, int64_t* out_idx, double* out_dist, int64_t cap,
+                 int64_t* out_count, fsmeld_counters* counters) {
+    return single(c, 2, query, m, cutoff, 0, metric, w, arg, eb, ee, out_idx, out_dist, cap, out_count,
+                  counters, nullptr);
+}
+
+int fsmeld_batch(fsmeld_ctx* c, int mode, const fsmeld_query* qs, int nq, fsmeld_result* res) {
+    if (!c || !qs || !res || nq < 0 || mode < 0 || mode > 2) return fail(FSMELD_E_ARG, "invalid batch");
+    FSM_CUDA_TRY(cudaSetDevice(c->device));
+    std::vector<HostQuery> hqs(nq);
+    std::vector<QueryRun> runs;
+    std::vector<int> map;
+    for (int i = 0; i < nq; ++i) {
+        res[i].count = 0;
+        res[i].status = prepare_query(qs[i].query, qs[i].m, qs[i].metric, qs[i].w, qs[i].arg, &hqs[i]);
+        if (res[i].status) continue;
+        if (mode == 1 && (qs[i].k < 1 || (long long)qs[i].k > c->n - qs[i].m + 1)) { res[i].status = FSMELD_E_ARG; continue; }
+        if (mode != 1 && !(std::isfinite(qs[i].cutoff) && qs[i].cutoff >= 0)) { res[i].status = FSMELD_E_ARG; continue; }
+        if (mode == 1 && res[i].capacity < qs[i].k) { res[i].status = FSMELD_E_ARG; continue; }
+        QueryRun qr{&hqs[i], mode, qs[i].cutoff, qs[i].k, qs[i].exclude_begin, qs[i].exclude_end,
+                    res[i].idx, res[i].dist, res[i].capacity, &res[i].count, &res[i].counters,
+                    res[i].seg_counts};
+        runs.push_back(qr);
+        map.push_back(i);
+    }
+    std::vector<int> st;
+    cudaEventRecord(c->ev0, c->stream);
+    int r = run_batch(c, runs, &st);
+    cudaEventRecord(c->ev1, c->stream);
+    cudaEventSynchronize(c->ev1);
+    for (size_t j = 0; j < map.size(); ++j) res[map[j]].status = st[j];
+    int first = r;
+    for (int i = 0; i < nq && !first; ++i) first = res[i].status;
+    return first;
+}
+
+int64_t fsmeld_inspect(fsmeld_ctx* c, const double* query, int m, int metric, int w, double arg, int what,
+                       double* out, int64_t cap) {
+    if (!c || !query || what < 0 || what > 5) return fail(FSMELD_E_ARG, "invalid inspect request");
+    FSM_CUDA_TRY(cudaSetDevice(c->device));
+    HostQuery hq;
+    int r = prepare_query(query, m, metric, w, arg, &hq);
+    if (r) return r;
+    Geom g;
+    if ((r = make_geom(c->n, m, -1, -1, &g))) return r;
+    Stats st;
+    if ((r = run_stats(c, g, &st, ""))) return r;
+    const double* src = nullptr;
+    long long count = 0;
+    if (what <= 1) {
+        src = what == 0 ? st.MU : st.SIG;
+        count = g.S * g.kml;
+    } else {
+        if ((r = run_env(c, g, w, &st, ""))) return r;
+        if (what <= 3) {
+            src = what == 2 ? st.Un : st.Ln;
+            count = g.S * g.m_k;
+        } else {
+            QueryDev qd;
+            if ((r = upload_query(c, hq, "query", &qd))) return r;
+            double* thr;
+            if ((r = bufT(c, "thr", (size_t)2 * g.S, &thr))) return r;
+            std::vector<ThrJob> jobs(1);
+            jobs[0].q = qd; jobs[0].Un = st.Un; jobs[0].Ln = st.Ln; jobs[0].thr = thr;
+            if ((r = run_thr(c, g, jobs))) return r;
+            if (what == 4) {
+                src = thr;
+                count = 2 * g.S;
+            } else {
+                unsigned long long* cnt;
+                if ((r = bufT(c, "counters", C_N, &cnt))) return r;
+                FSM_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, c->stream));
+                double* z;
+                if ((r = bufT(c, "zbuf", (size_t)g.S * g.kml, &z))) return r;
+                LbJob lj{};
+                lj.q = qd; lj.Un = st.Un; lj.Ln = st.Ln; lj.thr = thr; lj.SIG = st.SIG;
+                lj.zout = z; lj.nsurv = cnt + C_SURV; lj.nvalid = cnt + C_VALID;
+                if ((r = run_lbip(c, g, lj))) return r;
+                src = z;
+                count = g.S * g.kml;
+            }
+        }
+    }
+    const long long ncopy = std::min<long long>(count, cap);
+    if (out && ncopy > 0)
+        FSM_CUDA_TRY(cudaMemcpyAsync(out, src, sizeof(double) * ncopy, cudaMemcpyDeviceToHost, c->stream));
+    FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return count;
+}
+
+}  // extern "C"

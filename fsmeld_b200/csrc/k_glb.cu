@@ -1,0 +1,251 @@
+// GLB second filter (src/glb.cpp:200-373), split in the reference's own two
+// directions:
+//  * k_glb_tq: one lane per LB_IP survivor computes the boundary term and the
+//    T->Q sum with early abandon, z-normalising candidate points lazily
+//    (t - mu) / sigma exactly as src/fsmeld.cpp:823-826 does, so abandoned
+//    candidates never pay for the whole window;
+//  * k_glb_qt: one warp per T->Q survivor builds the candidate envelope
+//    (radius w, no NaN possible in a valid window) and the Q->T terms in
+//    parallel; lane 0 adds the terms in the reference's order, so the bound
+//    carries the reference's bits.
+// Early abandon compares a running sum of non-negative terms with the
+// cutoff; running sums never decrease, so testing the final sum once is the
+// same decision as testing after every term.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace fsm {
+
+namespace {
+
+__device__ __forceinline__ double edr_sub(double a, double b, double eps) {
+    return (fabs(dsub(a, b)) <= eps) ? 0.0 : 1.0;
+}
+__device__ __forceinline__ bool env_match(double v, double lo, double hi, double eps) {
+    if (v < lo) return dsub(lo, v) <= eps;
+    if (v > hi) return dsub(v, hi) <= eps;
+    return true;
+}
+__device__ __forceinline__ double dminv(double a, double b) { return (a < b) ? a : b; }  // MIN macro
+__device__ __forceinline__ double dmaxv(double a, double b) { return (a > b) ? a : b; }  // MAX macro
+
+// warp-aggregated append; returns nothing, writes entry via functor
+template <typename F>
+__device__ __forceinline__ void warp_append(bool pred, unsigned long long* counter, F write) {
+    const unsigned mask = __ballot_sync(0xffffffffu, pred);
+    if (!mask) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (pred) write(base + __popc(mask & ((1u << lane) - 1)));
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(256) k_glb_tq(Geom g, GlbJob job) {
+    extern __shared__ double gq_smem[];
+    const QueryDev& q = job.q;
+    const int m = q.m, metric = q.metric;
+    double* Q = gq_smem;
+    double* LQ = Q + m;
+    double* UQ = LQ + m;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) { Q[i] = q.qn[i]; LQ[i] = q.LQ[i]; UQ[i] = q.UQ[i]; }
+    __syncthreads();
+    const double bsf = q.cutoff;
+    const double sq = dmul(bsf, bsf);  // glb_exceeds_squared_bsf, src/glb.cpp:28-31
+    const double arg = q.arg;
+    const unsigned long long n_in = *job.n_in;
+    const unsigned long long n_lim = n_in < (unsigned long long)job.in_cap ? n_in : job.in_cap;
+    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < n_lim;
+         base += (unsigned long long)gridDim.x * blockDim.x) {
+        const unsigned long long idx = base + threadIdx.x;
+        const bool active = idx < n_lim;
+        long long gi = 0;
+        double mu = 0.0, sg = 1.0;
+        if (active) {
+            gi = job.in[idx];
+            long long s;
+            int j;
+            g.locate(gi, &s, &j);
+            mu = job.MU[s * g.kml + j];
+            sg = job.SIG[s * g.kml + j];
+        }
+        const double* tp = job.target + gi;
+        bool alive = active;
+        double boundary = 0.0, tq = 0.0;
+        if (active) {
+#define TN(k) ddiv(dsub(tp[(k)], mu), sg)
+            const double T0 = TN(0), TL = TN(m - 1);
+            switch (metric) {
+                case DTW:
+                    boundary = dadd(dsq(T0, Q[0]), dsq(TL, Q[m - 1]));
+                    for (int k = 1; k < m - 1; ++k) {
+                        const double t = TN(k);
+                        if (t < LQ[k]) tq = dadd(tq, dsq(t, LQ[k]));
+                        else if (t > UQ[k]) tq = dadd(tq, dsq(t, UQ[k]));
+                        if (dadd(boundary, tq) > sq) { alive = false; break; }
+                    }
+                    break;
+                case ERP:
+                    boundary = dmin3(dsq(Q[m - 1], TL), dsq(Q[m - 1], arg), dsq(TL, arg));
+                    for (int k = 1; k < m - 1; ++k) {
+                        const double t = TN(k);
+                        if (t > UQ[k]) tq = dadd(tq, dminv(dsq(t, UQ[k]), dsq(t, arg)));
+                        else if (t < LQ[k]) tq = dadd(tq, dminv(dsq(t, LQ[k]), dsq(t, arg)));
+                        if (dadd(boundary, tq) > sq) { alive = false; break; }
+                    }
+                    break;
+                case EDR:
+                    boundary = dminv(edr_sub(Q[m - 1], TL, arg), 1.0);
+                    for (int k = 1; k < m - 1; ++k) {
+                        const double t = TN(k);
+                        if (t > UQ[k]) tq = dadd(tq, edr_sub(t, UQ[k], arg));
+                        else if (t < LQ[k]) tq = dadd(tq, edr_sub(t, LQ[k], arg));
+                        if (dadd(boundary, tq) > bsf) { alive = false; break; }
+                    }
+                    break;
+                case LCSS: {
+                    const double min_len = (double)m;
+                    for (int k = 0; k < m; ++k) {
+                        const double t = (k == 0) ? T0 : ((k == m - 1) ? TL : TN(k));
+                        if (env_match(t, LQ[k], UQ[k], arg)) tq = dadd(tq, 1.0);
+                    }
+                    if (dmax0(dsub(1.0, ddiv(tq, min_len))) > bsf) alive = false;
+                    break;
+                }
+                default: {  // MSM
+                    const double T2 = TN(m - 2);
+                    const double q0 = Q[0], ql = Q[m - 1], ql2 = Q[m - 2];
+                    if ((T2 >= TL && TL >= ql) || (T2 <= TL && TL <= ql) || (ql2 <= ql && ql <= TL) ||
+                        (ql2 >= ql && ql >= TL)) {
+                        boundary = dadd(fabs(dsub(q0, T0)), dminv(fabs(dsub(ql, TL)), arg));
+                    } else {
+                        boundary = dadd(fabs(dsub(q0, T0)),
+                                        dmin3(fabs(dsub(ql, TL)), dadd(arg, fabs(dsub(TL, T2))),
+                                              dadd(arg, fabs(dsub(ql, ql2)))));
+                    }
+                    for (int k = 1; k < m - 1; ++k) {
+                        const double t = TN(k);
+                        if (t > UQ[k]) tq = dadd(tq, dminv(fabs(dsub(t, UQ[k])), arg));
+                        else if (t < LQ[k]) tq = dadd(tq, dminv(fabs(dsub(t, LQ[k])), arg));
+                        if (dadd(boundary, tq) > bsf) { alive = false; break; }
+                    }
+                    break;
+                }
+            }
+#undef TN
+        }
+        if (active && !alive) {
+            // abandoned: GLB returns MAX_VAL (src/glb.cpp:221 etc.); it survives only if
+            // MAX_VAL <= cutoff
+            if (kGlbMax <= bsf) alive = true, boundary = -1.0;  // marker: keep as MAX_VAL
+        }
+        warp_append(alive, job.n_out, [&](unsigned long long o) {
+            if (o < (unsigned long long)job.out_cap) {
+                job.out[o] = gi;
+                job.out_b[o] = boundary;
+                job.out_t[o] = tq;
+            }
+        });
+    }
+}
+
+// one warp per T->Q survivor
+__global__ void __launch_bounds__(256) k_glb_qt(Geom g, GlbJob job) {
+    extern __shared__ double gqt_smem[];
+    const QueryDev& q = job.q;
+    const int m = q.m, metric = q.metric, w = q.w;
+    const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double* Q = gqt_smem;
+    double* Tw = Q + m + warp * 2 * m;   // normalised candidate
+    double* term = Tw + m;               // Q->T terms
+    for (int i = threadIdx.x; i < m; i += blockDim.x) Q[i] = q.qn[i];
+    __syncthreads();
+    const double bsf = q.cutoff;
+    const double sq = dmul(bsf, bsf);
+    const double arg = q.arg;
+    const unsigned long long n_in = *job.n_in;
+    const unsigned long long n_lim = n_in < (unsigned long long)job.in_cap ? n_in : job.in_cap;
+    for (unsigned long long c = (unsigned long long)blockIdx.x * warps + warp; c < n_lim;
+         c += (unsigned long long)gridDim.x * warps) {
+        const long long gi = job.in[c];
+        const double boundary = job.in_b[c];
+        const double tq = job.in_t[c];
+        long long s;
+        int j;
+        g.locate(gi, &s, &j);
+        double glb;
+        if (boundary == -1.0) {
+            glb = kGlbMax;  // abandoned in T->Q but MAX_VAL <= cutoff
+        } else {
+            const double mu = job.MU[s * g.kml + j], sg = job.SIG[s * g.kml + j];
+            const double* tp = job.target + gi;
+            for (int k = lane; k < m; k += 32) Tw[k] = ddiv(dsub(tp[k], mu), sg);
+            __syncwarp();
+            // candidate envelope (src/glb.cpp:302-304 -> src/lower_upper_lemire.cpp:8-44)
+            double qr = 0.0;
+            for (int k = lane; k < m; k += 32) {
+                const int a = max(0, k - w), b = min(m - 1, k + w);
+                double lo = Tw[a], hi = Tw[a];
+                for (int i = a + 1; i <= b; ++i) {
+                    const double v = Tw[i];
+                    lo = (v <= lo) ? v : lo;
+                    hi = (v >= hi) ? v : hi;
+                }
+                const double x = Q[k];
+                double tm = 0.0;
+                switch (metric) {
+                    case DTW:
+                        if (x < lo) tm = dsq(x, lo);
+                        else if (x > hi) tm = dsq(x, hi);
+                        break;
+                    case ERP:
+                        if (x > hi) tm = dminv(dsq(x, hi), dsq(x, arg));
+                        else if (x < lo) tm = dminv(dsq(x, lo), dsq(x, arg));
+                        break;
+                    case EDR:
+                        if (x > hi) tm = edr_sub(x, hi, arg);
+                        else if (x < lo) tm = edr_sub(x, lo, arg);
+                        break;
+                    case LCSS:
+                        tm = env_match(x, lo, hi, arg) ? 1.0 : 0.0;
+                        break;
+                    default:
+                        if (x > hi) tm = dminv(fabs(dsub(x, hi)), arg);
+                        else if (x < lo) tm = dminv(fabs(dsub(x, lo)), arg);
+                        break;
+                }
+                term[k] = tm;
+                if (metric == LCSS) qr += tm;
+            }
+            __syncwarp();
+            if (metric == LCSS) {
+                for (int o = 16; o; o >>= 1) qr += __shfl_xor_sync(0xffffffffu, qr, o);
+                const double min_len = (double)m;
+                glb = dmax0(dsub(1.0, ddiv(dminv(tq, qr), min_len)));
+            } else {
+                double qt = 0.0;
+                if (lane == 0)
+                    for (int k = 1; k < m - 1; ++k) qt = dadd(qt, term[k]);
+                qt = __shfl_sync(0xffffffffu, qt, 0);
+                const double tot = dadd(boundary, qt);
+                if (metric == DTW || metric == ERP) {
+                    glb = (tot > sq) ? kGlbMax : dsqrt(dmax0(dadd(boundary, dmaxv(tq, qt))));
+                } else {
+                    glb = (tot > bsf) ? kGlbMax : dadd(boundary, dmaxv(tq, qt));
+                }
+            }
+            __syncwarp();
+        }
+        const bool keep = glb <= bsf;
+        if (lane == 0 && keep) {
+            const unsigned long long o = atomicAdd(job.n_out, 1ull);
+            if (o < (unsigned long long)job.out_cap) job.out[o] = gi;
+            if (job.segc && s < g.forsize) atomicAdd((unsigned long long*)&job.segc[3 * s + 2], 1ull);
+        }
+    }
+}
+
+}  // namespace fsm

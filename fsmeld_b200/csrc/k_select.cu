@@ -1,0 +1,89 @@
+// Candidate selection for the top-k `cutoff` command (src/fsmeld.cpp:185-569).
+//
+// The reference scans candidates in index order with a k-element max-heap of
+// (distance, index) pairs and a threshold that tightens as the heap fills;
+// since replacement needs a strictly smaller distance and indices arrive in
+// increasing order, its result is exactly the k lexicographically smallest
+// (distance, index) pairs among valid candidates.  The device form reaches
+// the same set without the serial scan:
+//  1. LB_IP per window (k_lbip with z output);
+//  2. seeds: the window with the smallest LB of each segment (k_seg_argmin);
+//     the k-th smallest exact distance among the best seeds is an upper
+//     bound tau on the k-th smallest distance overall;
+//  3. every valid window whose LB does not exceed tau (k_lb_filter) goes
+//     through GLB at tau and then the exact DP; any window whose distance is
+//     at most the true k-th distance survives both admissible bounds;
+//  4. a lexicographic sort of the surviving (distance, index) pairs gives the
+//     ranking and the threshold.
+#include <cub/block/block_reduce.cuh>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace fsm {
+
+__global__ void __launch_bounds__(256) k_lb_filter(Geom g, const double* __restrict__ z,
+                                                   const double* __restrict__ SIG, double cutoff,
+                                                   int metric, long long* out, unsigned long long* n_out,
+                                                   long long cap) {
+    const int lane = threadIdx.x & 31;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < g.tsn;
+         base += (long long)gridDim.x * blockDim.x) {
+        const long long gi = base + threadIdx.x;
+        bool keep = false;
+        if (gi < g.tsn) {
+            long long s;
+            int j;
+            g.locate(gi, &s, &j);
+            const double sg = SIG[s * g.kml + j];
+            keep = !window_invalid(sg, g, gi) && !lbip_exceeds(z[s * g.kml + j], cutoff, metric);
+        }
+        const unsigned mask = __ballot_sync(0xffffffffu, keep);
+        if (mask) {
+            unsigned long long o = 0;
+            const int leader = __ffs(mask) - 1;
+            if (lane == leader) o = atomicAdd(n_out, (unsigned long long)__popc(mask));
+            o = __shfl_sync(0xffffffffu, o, leader) + __popc(mask & ((1u << lane) - 1));
+            if (keep && o < (unsigned long long)cap) out[o] = gi;
+        }
+    }
+}
+
+struct MinZ {
+    double z;
+    long long gi;
+};
+struct MinZOp {
+    __device__ MinZ operator()(const MinZ& a, const MinZ& b) const {
+        if (a.z < b.z) return a;
+        if (b.z < a.z) return b;
+        return (a.gi <= b.gi) ? a : b;
+    }
+};
+
+// one block per segment: the valid window with the smallest LB (ties: lowest index)
+__global__ void __launch_bounds__(256) k_seed(Geom g, const double* __restrict__ z,
+                                              const double* __restrict__ SIG, int per_seg,
+                                              long long* out, unsigned long long* n_out, long long cap) {
+    using Red = cub::BlockReduce<MinZ, 256>;
+    __shared__ typename Red::TempStorage tmp;
+    (void)per_seg;
+    for (long long s = blockIdx.x; s < g.S; s += gridDim.x) {
+        MinZ best{INFINITY, -1};
+        for (int j = g.lo(s) + threadIdx.x; j < g.kml; j += blockDim.x) {
+            const long long gi = g.gidx(s, j);
+            if (window_invalid(SIG[s * g.kml + j], g, gi)) continue;
+            double zz = z[s * g.kml + j];
+            if (isnan(zz)) zz = INFINITY;
+            best = MinZOp()(best, MinZ{zz, gi});
+        }
+        const MinZ r = Red(tmp).Reduce(best, MinZOp());
+        if (threadIdx.x == 0 && r.gi >= 0) {
+            const unsigned long long o = atomicAdd(n_out, 1ull);
+            if (o < (unsigned long long)cap) out[o] = r.gi;
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace fsm

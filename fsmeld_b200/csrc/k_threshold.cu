@@ -1,0 +1,494 @@
+// LB_IP threshold selection per macro segment and side
+// (src/find_t_lp.cpp: find_tl_lp_dtw 218-287, find_tl_lp 288-398,
+//  find_tl_lp_erp 510-582, find_tu_lp_erp 583-654, find_tu_lp_dtw 655-724,
+//  find_tu_lp 726-825; dispatch src/fsmeld.cpp:778-790).
+//
+// The reference: run-length dedup of the envelope core U/L_normal[m-1 ..
+// m_k-m] (consecutive equal values only), sort, then one sequential sweep
+// that moves pointers over the sorted query, updates running power sums m_p
+// and a penalty sum C, and scores LB[i] = h(t_i) * g_i; the argmax gives t.
+//
+// Here one CTA handles one (segment, side):
+//  1. dedup with a block scan, sort runs with a block merge sort (total
+//     order: value, NaN last, ties by position);
+//  2. every pointer move of the sweep becomes an op with the sweep step at
+//     which it fires (a binary search over the sorted values); ops are
+//     ordered by (step, stream, rank) -- the order the reference's loops
+//     perform them in;
+//  3. one thread replays the ops in that order, so m_p and C carry the
+//     reference's rounding bit for bit, and records the state after each op;
+//  4. every candidate reads its state, scores LB in parallel, and a block
+//     reduction takes the first maximum (NaN at index 0 wins, as in
+//     findMaxIndex, src/find_t_lp.cpp:206-216).
+// ERP's priority queues pop equal keys in an order the C++ library leaves
+// to its heap layout; here equal keys pop by query index.  The threshold is
+// the same unless two candidates' scores tie to the last bit.
+#include <climits>
+#include <cub/block/block_merge_sort.cuh>
+#include <cub/block/block_reduce.cuh>
+#include <cub/block/block_scan.cuh>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace fsm {
+
+namespace {
+
+constexpr int kNever = INT_MAX;
+
+struct RunKey {
+    double v;
+    int pos;
+    int cnt;
+};
+
+struct RunLess {
+    int desc;
+    __device__ bool operator()(const RunKey& a, const RunKey& b) const {
+        const bool na = isnan(a.v), nb = isnan(b.v);
+        if (na != nb) return nb;
+        if (!na) {
+            if (desc) {
+                if (a.v > b.v) return true;
+                if (a.v < b.v) return false;
+            } else {
+                if (a.v < b.v) return true;
+                if (a.v > b.v) return false;
+            }
+        }
+        return a.pos < b.pos;
+    }
+};
+
+struct ArgMax {
+    double v;
+    int i;
+    int ok;  // 0 for NaN scores (never selected unless at index 0)
+};
+struct ArgMaxOp {
+    __device__ ArgMax operator()(const ArgMax& a, const ArgMax& b) const {
+        if (!a.ok) return b;
+        if (!b.ok) return a;
+        if (a.v > b.v) return a;
+        if (b.v > a.v) return b;
+        return (a.i <= b.i) ? a : b;
+    }
+};
+
+enum Cmp { LE, LT, GE, GT };
+
+// first i in [0, n) with tv[i] (cmp) x, or kNever; tv is monotone so the
+// predicate is false..false true..true
+__device__ __forceinline__ int first_step(const double* tv, int n, Cmp c, double x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        const double t = tv[mid];
+        bool p;
+        switch (c) {
+            case LE: p = t <= x; break;
+            case LT: p = t < x; break;
+            case GE: p = t >= x; break;
+            default: p = t > x; break;
+        }
+        if (p) hi = mid; else lo = mid + 1;
+    }
+    return lo < n ? lo : kNever;
+}
+
+__device__ __forceinline__ int lower_count(const double* a, int n, double x) {  // #(a < x), a ascending
+    int lo = 0, hi = n;
+    while (lo < hi) { const int mid = (lo + hi) >> 1; if (a[mid] < x) lo = mid + 1; else hi = mid; }
+    return lo;
+}
+__device__ __forceinline__ int upper_count(const double* a, int n, double x) {  // #(a <= x)
+    int lo = 0, hi = n;
+    while (lo < hi) { const int mid = (lo + hi) >> 1; if (a[mid] <= x) lo = mid + 1; else hi = mid; }
+    return lo;
+}
+// prefix length of an index-ordered table whose keys satisfy pred (monotone)
+template <typename F>
+__device__ __forceinline__ int prefix_count(int n, F pred) {
+    int lo = 0, hi = n;
+    while (lo < hi) { const int mid = (lo + hi) >> 1; if (pred(mid)) lo = mid + 1; else hi = mid; }
+    return lo;
+}
+
+__device__ __forceinline__ double f_p(double mp0, double mp1, double mp2, int p, double t) {
+    // src/find_t_lp.cpp:187-199 (p == 0 only occurs for EDR/LCSS, which return 0)
+    if (p == 0) return 0.0;
+    if (p == 1) return dsub(mp1, dmul(mp0, t));
+    return dadd(dsub(mp2, dmul(dmul(mp1, t), 2.0)), dmul(mp0, dmul(t, t)));
+}
+
+// Stream plan of one (metric, side): op element, step, payload kind.
+struct Plan {
+    int kind;      // 0 DTW, 1 general (MSM, EDR, LCSS), 2 ERP
+    int upper;
+    int idx1, idx2, kA0, kB0;
+    int nA, nB;
+    int p;
+};
+
+}  // namespace
+
+template <int T, int IPT>
+__global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restrict__ jobs,
+                                                 unsigned char* gwork, long long slot_stride) {
+    using Sort = cub::BlockMergeSort<RunKey, T, IPT>;
+    using IScan = cub::BlockScan<int, T>;
+    using AReduce = cub::BlockReduce<ArgMax, T>;
+    constexpr int CAP = T * IPT;
+
+    extern __shared__ __align__(16) unsigned char thr_smem[];
+    __shared__ typename IScan::TempStorage iscan_tmp;
+    __shared__ typename AReduce::TempStorage red_tmp;
+    __shared__ int s_nr, s_nfin, s_best, s_nops;
+    __shared__ Plan s_plan;
+    __shared__ double s_t0;
+
+    const ThrJob& job = jobs[blockIdx.y];
+    const QueryDev& q = job.q;
+    const int m = q.m, mk = g.m_k;
+    const int cnt = mk - 2 * m + 2;
+    const int t = threadIdx.x;
+
+    unsigned char* base = gwork ? gwork + (long long)(blockIdx.y * gridDim.x + blockIdx.x) * slot_stride
+                                : thr_smem;
+    // region X: runs (phase 1) / sort temp (phase 2) / sorted values + g (phase 3)
+    const size_t xbytes = ((sizeof(typename Sort::TempStorage) > (size_t)CAP * 16 + 16
+                                ? sizeof(typename Sort::TempStorage)
+                                : (size_t)CAP * 16 + 16) + 15) & ~size_t(15);
+    double* rval = (double*)base;                       // [CAP]
+    int* rstart = (int*)(base + (size_t)CAP * 8);       // [CAP + 1]
+    typename Sort::TempStorage& sort_tmp = *reinterpret_cast<typename Sort::TempStorage*>(base);
+    double* tv = (double*)base;                         // [CAP] sorted values
+    int* gp = (int*)(base + (size_t)CAP * 8);           // [CAP] inclusive count sums
+    unsigned char* zb = base + xbytes;
+    int* sA = (int*)zb;                                 // [m]
+    int* sB = sA + m;                                   // [m]
+    int* opdesc = sB + m;                               // [2m]
+    int* opstep = opdesc + 2 * m;                       // [2m]
+    double* st = (double*)(((uintptr_t)(opstep + 2 * m) + 15) & ~uintptr_t(15));  // [(2m+1)*4]
+
+    const int p = q.p;
+    const int kind = (q.metric == DTW) ? 0 : (q.metric == ERP ? 2 : 1);
+
+    for (long long bid = blockIdx.x; bid < 2 * g.S; bid += gridDim.x) {
+        const long long s = bid >> 1;
+        const int upper = (int)(bid & 1);
+        const double* env = (upper ? job.Un : job.Ln) + s * mk + (m - 1);
+
+        // ---- 1. run-length dedup (src/find_t_lp.cpp:53-67)
+        double v[IPT];
+        int nflag = 0;
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            const int i = t * IPT + k;
+            v[k] = (i < cnt) ? env[i] : 0.0;
+        }
+        bool flag[IPT];
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            const int i = t * IPT + k;
+            bool f = false;
+            if (i < cnt) {
+                const double prev = (k > 0) ? v[k - 1] : (i > 0 ? env[i - 1] : 0.0);
+                f = (i == 0) || (v[k] != prev);
+            }
+            flag[k] = f;
+            nflag += f ? 1 : 0;
+        }
+        int roff, nr;
+        IScan(iscan_tmp).ExclusiveSum(nflag, roff, nr);
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            if (flag[k]) {
+                rstart[roff] = t * IPT + k;
+                rval[roff] = v[k];
+                ++roff;
+            }
+        }
+        if (t == 0) { rstart[nr] = cnt; s_nr = nr; }
+        __syncthreads();
+
+        // ---- 2. sort runs (src/find_t_lp.cpp:68-81)
+        RunKey keys[IPT];
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            const int r = t * IPT + k;
+            if (r < nr) keys[k] = RunKey{rval[r], r, rstart[r + 1] - rstart[r]};
+            else keys[k] = RunKey{dnan(), INT_MAX, 0};
+        }
+        __syncthreads();
+        Sort(sort_tmp).Sort(keys, RunLess{upper ? 0 : 1}, nr, RunKey{dnan(), INT_MAX, 0});
+        __syncthreads();
+
+        // ---- 3. sorted values, cumulative counts g_i, finite prefix length
+        int csum = 0, nf = 0;
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            const int i = t * IPT + k;
+            if (i < nr) { csum += keys[k].cnt; nf += isnan(keys[k].v) ? 0 : 1; }
+        }
+        int cbase;
+        IScan(iscan_tmp).ExclusiveSum(csum, cbase);
+        __syncthreads();
+        int nfin_total;
+        IScan(iscan_tmp).ExclusiveSum(nf, nf, nfin_total);
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            const int i = t * IPT + k;
+            if (i < nr) {
+                tv[i] = keys[k].v;
+                cbase += keys[k].cnt;
+                gp[i] = cbase;
+            }
+        }
+        if (t == 0) s_nfin = nfin_total;
+        __syncthreads();
+        const int nfin = s_nfin;
+        double* out = job.thr + s * 2 + upper;
+        if (nfin == 0) {  // every score is NaN: index 0 wins
+            if (t == 0) *out = tv[0];
+            __syncthreads();
+            continue;
+        }
+
+        // ---- 4. stream plan (one thread), src/find_t_lp.cpp init loops
+        if (t == 0) {
+            const double t0 = tv[0];
+            Plan pl;
+            pl.kind = kind; pl.upper = upper; pl.p = p;
+            pl.idx1 = pl.idx2 = pl.kA0 = pl.kB0 = 0;
+            pl.nA = pl.nB = 0;
+            if (kind == 0) {
+                if (!upper) { pl.idx1 = lower_count(q.qs, m, t0) - 1; pl.nB = pl.idx1 + 1; }
+                else { pl.idx1 = upper_count(q.qs, m, t0); pl.nB = m - pl.idx1; }
+            } else if (kind == 1) {
+                if (!upper) {
+                    pl.idx1 = lower_count(q.qs, m, t0) - 1;
+                    pl.idx2 = min(pl.idx1, lower_count(q.tlq, m, t0) - 1);
+                    pl.nA = pl.idx2 + 1;
+                    pl.nB = pl.idx1 + 1;
+                } else {
+                    pl.idx1 = upper_count(q.qs, m, t0);
+                    pl.idx2 = max(pl.idx1, upper_count(q.tuq, m, t0));
+                    pl.nA = m - pl.idx2;
+                    pl.nB = m - pl.idx1;
+                }
+            } else {
+                if (!upper) {
+                    const int* oa = q.ordA_l;
+                    const int* ob = q.ordB_l;
+                    pl.kA0 = prefix_count(m, [&](int k) { return q.otl[oa[k]] >= t0; });
+                    pl.kB0 = prefix_count(m, [&](int k) { return q.qn[ob[k]] >= t0; });
+                } else {
+                    const int* oa = q.ordA_u;
+                    const int* ob = q.ordB_u;
+                    pl.kA0 = prefix_count(m, [&](int k) { return q.otu[oa[k]] <= t0; });
+                    pl.kB0 = prefix_count(m, [&](int k) { return q.qn[ob[k]] <= t0; });
+                }
+                pl.nA = m - pl.kA0;
+                pl.nB = m - pl.kB0;
+            }
+            s_plan = pl;
+            s_t0 = t0;
+        }
+        __syncthreads();
+        const Plan pl = s_plan;
+        const double t0 = s_t0;
+
+        // ---- 5. firing step of every op
+        for (int r = t; r < pl.nA; r += T) {
+            int st_ = kNever;
+            if (kind == 1) {
+                if (!upper) { const int j = pl.idx2 - r; st_ = first_step(tv, nfin, LE, q.tlq[j]); }
+                else { const int j = pl.idx2 + r; st_ = first_step(tv, nfin, GE, q.tuq[j]); }
+            } else if (kind == 2) {
+                if (!upper) { const int e = q.ordA_l[pl.kA0 + r]; st_ = first_step(tv, nfin, LE, q.otl[e]); }
+                else { const int e = q.ordA_u[pl.kA0 + r]; st_ = first_step(tv, nfin, GE, q.otu[e]); }
+            }
+            sA[r] = st_;
+        }
+        for (int r = t; r < pl.nB; r += T) {
+            int st_ = kNever;
+            if (kind == 0) {
+                if (!upper) st_ = first_step(tv, nfin, LE, q.qs[pl.idx1 - r]);
+                else st_ = first_step(tv, nfin, GT, q.qs[pl.idx1 + r]);
+            } else if (kind == 1) {
+                if (!upper) {
+                    const int j = pl.idx1 - r;
+                    st_ = first_step(tv, nfin, LT, q.qs[j]);
+                    if (j <= pl.idx2 && st_ != kNever) st_ = max(st_, first_step(tv, nfin, LE, q.tlq[j]));
+                } else {
+                    const int j = pl.idx1 + r;
+                    st_ = first_step(tv, nfin, GT, q.qs[j]);
+                    if (j >= pl.idx2 && st_ != kNever) st_ = max(st_, first_step(tv, nfin, GE, q.tuq[j]));
+                }
+            } else {
+                if (!upper) {
+                    const int e = q.ordB_l[pl.kB0 + r];
+                    st_ = first_step(tv, nfin, LE, q.qn[e]);
+                    if (q.otl[e] < t0 && st_ != kNever) st_ = max(st_, first_step(tv, nfin, LE, q.otl[e]));
+                } else {
+                    const int e = q.ordB_u[pl.kB0 + r];
+                    st_ = first_step(tv, nfin, GE, q.qn[e]);
+                    if (q.otu[e] > t0 && st_ != kNever) st_ = max(st_, first_step(tv, nfin, GE, q.otu[e]));
+                }
+            }
+            sB[r] = st_;
+        }
+        __syncthreads();
+
+        // ---- 6. op order: (step, stream A before B, rank)
+        // valid ops form a prefix of each stream (steps never go from finite to kNever and back)
+        const int nAv = prefix_count(pl.nA, [&](int r) { return sA[r] != kNever; });
+        const int nBv = prefix_count(pl.nB, [&](int r) { return sB[r] != kNever; });
+        const bool b_sorted = (kind != 2);
+        for (int k = t; k < nAv + nBv; k += T) opdesc[k] = -1;
+        __syncthreads();
+        for (int r = t; r < nAv; r += T) {
+            const int sa = sA[r];
+            int blt;  // valid B ops with step < sa
+            if (b_sorted) {
+                blt = prefix_count(nBv, [&](int k) { return sB[k] < sa; });
+            } else {
+                blt = 0;
+                for (int k = 0; k < nBv; ++k) blt += (sB[k] < sa) ? 1 : 0;
+            }
+            const int pos = r + blt;
+            opdesc[pos] = r;
+            opstep[pos] = sa;
+        }
+        for (int r = t; r < nBv; r += T) {
+            const int sb = sB[r];
+            int bbefore;
+            if (b_sorted) {
+                bbefore = r;
+            } else {
+                bbefore = 0;
+                for (int k = 0; k < nBv; ++k) {
+                    const int sk = sB[k];
+                    bbefore += (sk < sb || (sk == sb && k < r)) ? 1 : 0;
+                }
+            }
+            const int ale = prefix_count(nAv, [&](int k) { return sA[k] <= sb; });
+            const int pos = bbefore + ale;
+            opdesc[pos] = 0x40000000 | r;
+            opstep[pos] = sb;
+        }
+        if (t == 0) s_nops = nAv + nBv;
+        __syncthreads();
+        const int nops = s_nops;
+
+        // ---- 7. replay: initial sums then every op, in the reference's order
+        if (t == 0) {
+            double mp0 = 0.0, mp1 = 0.0, mp2 = 0.0, C = 0.0;
+            const double* pw0 = (kind == 2) ? q.opw : q.pw;
+            const double* pw1 = pw0 + m;
+            const double* pw2 = pw0 + 2 * m;
+            if (kind == 0) {
+                if (!upper) { for (int j = 0; j <= pl.idx1; ++j) { mp0 = dadd(mp0, pw0[j]); mp1 = dadd(mp1, pw1[j]); mp2 = dadd(mp2, pw2[j]); } }
+                else { for (int j = pl.idx1; j < m; ++j) { mp0 = dadd(mp0, pw0[j]); mp1 = dadd(mp1, pw1[j]); mp2 = dadd(mp2, pw2[j]); } }
+            } else if (kind == 1) {
+                if (!upper) {
+                    for (int j = pl.idx1; j > pl.idx2; --j) { mp0 = dadd(mp0, pw0[j]); mp1 = dadd(mp1, pw1[j]); mp2 = dadd(mp2, pw2[j]); }
+                    for (int j = 0; j <= pl.idx2; ++j) C = dadd(C, q.Dq[j]);
+                } else {
+                    for (int j = pl.idx1; j < pl.idx2; ++j) { mp0 = dadd(mp0, pw0[j]); mp1 = dadd(mp1, pw1[j]); mp2 = dadd(mp2, pw2[j]); }
+                    for (int j = pl.idx2; j < m; ++j) C = dadd(C, q.Dq[j]);
+                }
+            } else {
+                for (int e = 0; e < m; ++e) {
+                    const double qv = q.qn[e];
+                    if (!upper) {
+                        if (qv >= t0) continue;
+                        if (q.otl[e] >= t0) { mp0 = dadd(mp0, pw0[e]); mp1 = dadd(mp1, pw1[e]); mp2 = dadd(mp2, pw2[e]); }
+                        else C = dadd(C, q.oD[e]);
+                    } else {
+                        if (qv <= t0) continue;
+                        if (q.otu[e] <= t0) { mp0 = dadd(mp0, pw0[e]); mp1 = dadd(mp1, pw1[e]); mp2 = dadd(mp2, pw2[e]); }
+                        else C = dadd(C, q.oD[e]);
+                    }
+                }
+            }
+            st[0] = mp0; st[1] = mp1; st[2] = mp2; st[3] = C;
+            for (int k = 0; k < nops; ++k) {
+                const int d = opdesc[k];
+                double* o = st + 4 * (k + 1);
+                if (d < 0) {  // unreachable when the op order is a permutation; keeps reads in bounds
+                    o[0] = mp0; o[1] = mp1; o[2] = mp2; o[3] = C;
+                    continue;
+                }
+                const int r = d & 0x3fffffff;
+                int x;  // table index of the op's query element
+                if (kind == 2) x = (d & 0x40000000) ? (upper ? q.ordB_u : q.ordB_l)[pl.kB0 + r]
+                                                    : (upper ? q.ordA_u : q.ordA_l)[pl.kA0 + r];
+                else if (d & 0x40000000) x = upper ? pl.idx1 + r : pl.idx1 - r;
+                else x = upper ? pl.idx2 + r : pl.idx2 - r;
+                x = min(max(x, 0), m - 1);
+                if (d & 0x40000000) {
+                    mp0 = dsub(mp0, pw0[x]); mp1 = dsub(mp1, pw1[x]); mp2 = dsub(mp2, pw2[x]);
+                } else {
+                    C = dsub(C, (kind == 2) ? q.oD[x] : q.Dq[x]);
+                    mp0 = dadd(mp0, pw0[x]); mp1 = dadd(mp1, pw1[x]); mp2 = dadd(mp2, pw2[x]);
+                }
+                o[0] = mp0; o[1] = mp1; o[2] = mp2; o[3] = C;
+            }
+        }
+        __syncthreads();
+
+        // ---- 8. scores and first maximum
+        ArgMax best{0.0, INT_MAX, 0};
+        int nan0 = 0;
+        for (int i = t; i < nr; i += T) {
+            int lo = 0, hi = nops;  // ops with step <= i
+            while (lo < hi) { const int mid = (lo + hi) >> 1; if (opstep[mid] <= i) lo = mid + 1; else hi = mid; }
+            const double* sv = st + 4 * lo;
+            const double tt = tv[i];
+            const double f = f_p(sv[0], sv[1], sv[2], p, tt);
+            double h;
+            if (kind == 0) h = upper ? f : fabs(f);
+            else h = dadd(sv[3], upper ? f : fabs(f));
+            const double lb = dmul(h, (double)gp[i]);
+            if (isnan(lb)) {
+                if (i == 0) nan0 = 1;  // findMaxIndex never leaves a NaN at index 0
+            } else {
+                best = ArgMaxOp()(best, ArgMax{lb, i, 1});
+            }
+        }
+        const int any_nan0 = __syncthreads_or(nan0);
+        const ArgMax r = AReduce(red_tmp).Reduce(best, ArgMaxOp());
+        if (t == 0) s_best = any_nan0 ? 0 : (r.ok ? r.i : 0);
+        __syncthreads();
+        if (t == 0) *out = tv[s_best];
+        __syncthreads();
+    }
+}
+
+size_t threshold_work_bytes(int cap_items, size_t sort_tmp, int m) {
+    const size_t cap = (size_t)cap_items;
+    size_t x = ((sort_tmp > cap * 16 + 16 ? sort_tmp : cap * 16 + 16) + 15) & ~size_t(15);
+    size_t z = (size_t)m * 4 * 6 + 16 + (size_t)(2 * m + 1) * 4 * 8;
+    return x + z + 64;
+}
+
+template <int T, int IPT>
+size_t threshold_sort_tmp_bytes() {
+    return sizeof(typename cub::BlockMergeSort<RunKey, T, IPT>::TempStorage);
+}
+
+#define FSM_THR_INST(T, IPT)                                                              \
+    template __global__ void k_threshold<T, IPT>(Geom, const ThrJob*, unsigned char*,      \
+                                                 long long);                              \
+    template size_t threshold_sort_tmp_bytes<T, IPT>();
+FSM_THR_INST(128, 4)
+FSM_THR_INST(256, 4)
+FSM_THR_INST(256, 8)
+FSM_THR_INST(512, 8)
+FSM_THR_INST(1024, 8)
+FSM_THR_INST(1024, 16)
+
+}  // namespace fsm

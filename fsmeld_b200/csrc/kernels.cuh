@@ -1,0 +1,98 @@
+// Kernel entry points and their job descriptors.
+#pragma once
+
+#include "common.cuh"
+
+namespace fsm {
+
+struct ThrJob {
+    QueryDev q;
+    const double* Un;  // [S][m_k]
+    const double* Ln;
+    double* thr;       // [S][2]: (t_l, t_u) per segment
+};
+
+struct LbJob {
+    QueryDev q;
+    const double* Un;
+    const double* Ln;
+    const double* thr;
+    const double* SIG;          // window sigmas [S][kml] (validity)
+    double* zout;               // optional: LB per window [S][kml] (NaN if invalid)
+    long long* surv;            // optional: LB survivors (global window index)
+    long long surv_cap;
+    unsigned long long* nsurv;
+    unsigned long long* nvalid; // valid, non-excluded windows
+    long long* segc;            // optional: per segment (valid, after LB, after GLB)
+    unsigned char* gwork;       // global scratch when the FFT buffers exceed shared memory
+    long long slot_stride;
+};
+
+struct GlbJob {
+    QueryDev q;
+    const double* target;
+    const double* MU;
+    const double* SIG;
+    const long long* in;
+    const double* in_b;         // stage 2 input: boundary terms
+    const double* in_t;         // stage 2 input: T->Q sums (LCSS: T->Q reward)
+    const unsigned long long* n_in;
+    long long in_cap;
+    long long* out;
+    double* out_b;
+    double* out_t;
+    unsigned long long* n_out;
+    long long out_cap;
+    long long* segc;
+};
+
+struct DpJob {
+    QueryDev q;
+    const double* target;
+    const double* MU;
+    const double* SIG;
+    const long long* list;      // candidates, or null for windows [0, n_windows)
+    const unsigned long long* n_list;
+    long long list_cap;
+    long long n_windows;
+    int mode;                   // 0: keep dist <= cutoff; 1: keep every finite dist
+    double cutoff;
+    long long* out_idx;
+    double* out_dist;
+    unsigned long long* n_out;
+    long long out_cap;
+    unsigned long long* n_valid;
+    double* gwork;              // global band scratch when shared memory is too small
+};
+
+__global__ void k_mvmean(const double* __restrict__ target, Geom g, double* __restrict__ mu,
+                         double* __restrict__ sig);
+template <int T, int OPT>
+__global__ void k_envelope(const double* __restrict__ target, const double* __restrict__ MU,
+                           const double* __restrict__ SIG, Geom g, int w, double* __restrict__ Un,
+                           double* __restrict__ Ln, double* gwork, long long slot_stride);
+template <int T, int IPT>
+__global__ void k_threshold(Geom g, const ThrJob* __restrict__ jobs, unsigned char* gwork,
+                            long long slot_stride);
+template <int T>
+__global__ void k_lbip(Geom g, LbJob job, const double2* __restrict__ W, int P, int logP);
+__global__ void k_glb_tq(Geom g, GlbJob job);
+__global__ void k_glb_qt(Geom g, GlbJob job);
+template <int METRIC>
+__global__ void k_dp(Geom g, DpJob job);
+__global__ void k_lb_filter(Geom g, const double* __restrict__ z, const double* __restrict__ SIG,
+                            double cutoff, int metric, long long* out, unsigned long long* n_out,
+                            long long cap);
+__global__ void k_seed(Geom g, const double* __restrict__ z, const double* __restrict__ SIG, int per_seg,
+                       long long* out, unsigned long long* n_out, long long cap);
+
+size_t mvmean_smem_bytes();
+size_t envelope_work_bytes(int m_k);
+size_t threshold_work_bytes(int cap_items, size_t sort_tmp, int m);
+template <int T, int IPT>
+size_t threshold_sort_tmp_bytes();
+size_t lbip_smem_bytes(int P, int m_k, int m, int metric);
+int lbip_set_w16();
+size_t dp_warp_doubles(int w);
+
+}  // namespace fsm

@@ -1,0 +1,158 @@
+/*
+ * fsmeld_cuda.h -- C ABI of the B200 (sm_100a) implementation of FSMELD's
+ * exact z-normalised subsequence range search (LB_IP -> GLB -> ELD).
+ *
+ * The reference exposes no library interface: its boundary is the
+ * `fsmeld search|cutoff|exact` command (src/main.cpp:40-110) and three C++
+ * entry points that take file paths and print to stdout
+ * (include/funcs.h:64-72):
+ *
+ *   FSMELD(...)                 -> fsmeld_search, fsmeld_search_file
+ *   FSMELD_find_threshold(...)  -> fsmeld_cutoff, fsmeld_cutoff_file
+ *   FSMELD_exact(...)           -> fsmeld_exact,  fsmeld_exact_file
+ *
+ * The *_file entry points are drop-ins for those three functions: same
+ * arguments (paths, m, cutoff or k, metric tag, w, arg, optional exclusion
+ * interval), same stdout and CSV output.  The in-memory entry points below
+ * them are what an FFI binding calls: plain pointers and sizes, caller-owned
+ * host buffers, integer status codes (no exception crosses the ABI).
+ *
+ * Threading: a context owns one CUDA stream and its device buffers; calls on
+ * one context are serialised by the caller; different contexts are
+ * independent.
+ */
+#ifndef FSMELD_CUDA_H
+#define FSMELD_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define FSMELD_OK 0
+#define FSMELD_E_ARG (-1)        /* invalid argument (message in fsmeld_last_error) */
+#define FSMELD_E_CUDA (-2)       /* CUDA runtime error */
+#define FSMELD_E_NOMEM (-3)      /* device allocation failed or budget exceeded */
+#define FSMELD_E_SHORT (-4)      /* target shorter than 2*m-1 points */
+#define FSMELD_E_FEWER_K (-5)    /* fewer valid, non-excluded candidates than k */
+#define FSMELD_E_UNSUPPORTED (-6)
+#define FSMELD_E_IO (-7)         /* file could not be read */
+
+/* metric ids: the reference's MetricType values (include/funcs.h:10-18) */
+#define FSMELD_DTW 1
+#define FSMELD_EDR 2
+#define FSMELD_ERP 3
+#define FSMELD_LCSS 4
+#define FSMELD_MSM 5
+
+typedef struct fsmeld_ctx fsmeld_ctx;
+
+/* Counters of one query; names follow the reference's printed counters
+ * (src/fsmeld.cpp:981-996, 521-528, 1295-1306). */
+typedef struct {
+    int64_t valid;        /* kk1: valid, non-excluded candidates */
+    int64_t invalid;      /* invalid or excluded candidates */
+    int64_t after_lb;     /* kk2: candidates not pruned by LB_IP */
+    int64_t after_glb;    /* kk3: candidates not pruned by GLB */
+    int64_t exact_evals;  /* exact elastic distances computed */
+    int64_t matches;      /* matches (search/exact) or k (cutoff) */
+    double threshold;     /* cutoff used (search/exact) or final top-k threshold */
+    int32_t m_k;          /* macro-segment length 2^ceil(log2(8m)), clipped to n */
+    int32_t reserved;
+    int64_t segments;     /* full macro segments */
+    int64_t tail;         /* windows in the EOF-aligned tail segment */
+    double device_ms;     /* device time of the call (CUDA events) */
+} fsmeld_counters;
+
+/* one query of a batched call */
+typedef struct {
+    const double* query;  /* host, m raw (unnormalised) values */
+    int32_t m;
+    int32_t metric;       /* FSMELD_DTW .. FSMELD_MSM */
+    int32_t w;            /* Sakoe-Chiba radius, 0 <= w < m */
+    int32_t k;            /* cutoff mode: k; otherwise ignored */
+    double arg;           /* ERP gap g, EDR/LCSS epsilon, MSM cost c; 0 for DTW */
+    double cutoff;        /* search/exact: distance cutoff */
+    int64_t exclude_begin;/* optional half-open exclusion [begin,end) of */
+    int64_t exclude_end;  /* candidate starts; -1,-1 for none */
+} fsmeld_query;
+
+/* results of one query of a batched call (caller-owned buffers) */
+typedef struct {
+    int64_t* idx;         /* match / rank indices, ascending index (search,
+                             exact) or ascending (distance, index) (cutoff) */
+    double* dist;         /* optional: distances for idx (exact, cutoff) */
+    int64_t capacity;     /* entries available in idx (and dist) */
+    int64_t count;        /* out: entries produced (may exceed capacity) */
+    int32_t status;       /* out: FSMELD_OK or an error code */
+    int32_t reserved;
+    fsmeld_counters counters;  /* out */
+    int64_t* seg_counts;  /* optional (search): 3 * segments int64 entries,
+                             per full segment (valid, after_lb, after_glb) */
+} fsmeld_result;
+
+/* ---- context -------------------------------------------------------- */
+
+/* Copy a host target (n native-endian doubles) to device `device`. */
+int fsmeld_open(int device, const double* host_target, int64_t n, fsmeld_ctx** out);
+/* Read a target file (headerless doubles) into a new context. */
+int fsmeld_open_file(int device, const char* path, fsmeld_ctx** out);
+/* Use a target already resident in device memory (not copied, not freed). */
+int fsmeld_open_device(int device, const double* device_target, int64_t n, fsmeld_ctx** out);
+int fsmeld_close(fsmeld_ctx* ctx);
+int64_t fsmeld_target_length(const fsmeld_ctx* ctx);
+const char* fsmeld_last_error(const fsmeld_ctx* ctx);
+const char* fsmeld_strerror(int status);
+/* Cap on device workspace bytes (0 = no cap); exceeding it -> FSMELD_E_NOMEM. */
+int fsmeld_set_workspace_limit(fsmeld_ctx* ctx, int64_t bytes);
+/* Number of CUDA kernel launches issued by this context so far. */
+int64_t fsmeld_kernel_launches(const fsmeld_ctx* ctx);
+
+/* ---- single queries (src/fsmeld.cpp:570-1074, 185-569, 1075-1344) --- */
+
+int fsmeld_search(fsmeld_ctx* ctx, const double* query, int m, double cutoff, int metric, int w,
+                  double arg, int64_t exclude_begin, int64_t exclude_end, int64_t* out_idx,
+                  int64_t capacity, int64_t* out_count, fsmeld_counters* counters,
+                  int64_t* seg_counts);
+int fsmeld_cutoff(fsmeld_ctx* ctx, const double* query, int m, int k, int metric, int w,
+                  double arg, int64_t exclude_begin, int64_t exclude_end, int64_t* out_idx,
+                  double* out_dist, fsmeld_counters* counters);
+int fsmeld_exact(fsmeld_ctx* ctx, const double* query, int m, double cutoff, int metric, int w,
+                 double arg, int64_t exclude_begin, int64_t exclude_end, int64_t* out_idx,
+                 double* out_dist, int64_t capacity, int64_t* out_count,
+                 fsmeld_counters* counters);
+
+/* ---- batched queries: one call, many queries of mixed m, metric, w ---- */
+/* mode: 0 = search, 1 = cutoff (k from each query), 2 = exact */
+int fsmeld_batch(fsmeld_ctx* ctx, int mode, const fsmeld_query* queries, int nq,
+                 fsmeld_result* results);
+
+/* ---- diagnostics (no counterpart in the reference): per-stage device
+ * arrays of one query, for stage-by-stage comparison with a CPU model.
+ * what: 0 window means [S*kml], 1 window sigmas [S*kml], 2 U_normal
+ * [S*m_k], 3 L_normal [S*m_k], 4 thresholds (t_l, t_u) [2*S], 5 LB_IP per
+ * window [S*kml] (NaN for invalid windows); S counts the tail segment.
+ * Returns the number of doubles available (copies at most cap). ---- */
+int64_t fsmeld_inspect(fsmeld_ctx* ctx, const double* query, int m, int metric, int w, double arg,
+                       int what, double* out, int64_t cap);
+
+/* ---- drop-ins for the reference's entry points (include/funcs.h:64-72):
+ *      read TARGET.bin / QUERY.txt, print the reference's stdout lines and
+ *      append the experiment CSV.  tag is "dtw", "erp", "edr", "lcss" or
+ *      "msm".  Return FSMELD_OK or an error code (message on stderr). ---- */
+int fsmeld_search_file(const char* target_path, const char* query_path, int m, double cutoff,
+                       const char* tag, int w, double arg, int64_t exclude_begin,
+                       int64_t exclude_end);
+int fsmeld_cutoff_file(const char* target_path, const char* query_path, int m, int k,
+                       const char* tag, int w, double arg, int64_t exclude_begin,
+                       int64_t exclude_end);
+int fsmeld_exact_file(const char* target_path, const char* query_path, int m, double cutoff,
+                      const char* tag, int w, double arg, int64_t exclude_begin,
+                      int64_t exclude_end);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
