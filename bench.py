@@ -1,0 +1,410 @@
+"""Benchmark: FSMELD exact subsequence range search on B200.
+
+Workload (the single-GPU configuration the headline metric is quoted on):
+five queries per step, one per metric (DTW, ERP g=0, EDR eps=0.25, LCSS
+eps=0.25, MSM c=0.5), m=256, w=13, on a 2^24-point float64 random walk with
+200 sine/chirp motifs, NaN spans (0.1% of points) and flat runs; each
+query's cutoff is its k=50 exact distance (computed once, untimed).  A step
+is one batched `search` of the five queries through the LB_IP -> GLB -> ELD
+cascade.  The metric is candidates/s: valid windows scanned per second,
+summed over the step's queries.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank searches its own target
+partition (weak scaling, no data-path collective); timings are the max over
+ranks.  `--impl reference` times the reference's own CPU code (built from
+its sources against the project FFT shim, oracle/_ref) on bounded samples.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_POINTS = 1 << 24
+M, W, K_TOP = 256, 13, 50
+METRICS = [("dtw", 0.0), ("erp", 0.0), ("edr", 0.25), ("lcss", 0.25), ("msm", 0.5)]
+WORKLOAD = ("five queries (dtw; erp g=0; edr eps=0.25; lcss eps=0.25; msm c=0.5), m=256, w=13, "
+            "2^24-point float64 random walk + 200 motifs + NaN spans + flat runs; cutoff = k=50 exact distance")
+# k=50 exact distance of each query over the full rank-0 target (part of the
+# workload definition; the GPU arm re-derives them with its own `cutoff` and
+# records whether they agree, the CPU reference arm uses them as given).
+CUTOFFS = {"dtw": 2.80906383446946, "erp": 5.138604886191949, "edr": 48.0, "lcss": 0.265625,
+           "msm": 74.7957914893858}
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def make_workload(rank):
+    from fsmeld_b200.synth import query_from, walk_with_structure
+    t = walk_with_structure(N_POINTS, M, seed=2 + 7919 * rank)
+    rng = np.random.default_rng(1002 + rank)
+    queries = {}
+    for metric, _ in METRICS:
+        q, _s = query_from(t, M, rng)
+        queries[metric] = q
+    return t, queries
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = str(gpu_index)
+        try:
+            import torch
+            self.gpu = "GPU-" + str(torch.cuda.get_device_properties(gpu_index).uuid)
+        except Exception:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            if vis:
+                self.gpu = vis.split(",")[gpu_index].strip()
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = []
+        mx = None
+        reasons = set()
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+                for nm, v in zip(names, r[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def load_peaks():
+    try:
+        with open(PEAKS_PATH) as f:
+            p = json.load(f)
+        return {"hbm_gbs": float(p["hbm_gbs"]), "bf16_tflops": float(p["bf16_tflops"]), "source": "measured"}
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+def roofline(stage, dominant, geom, peaks, n_queries):
+    """Algorithmic bytes per launch of the dominant kernel over its average launch time."""
+    name, (ms, launches) = dominant
+    S, m_k, kml = geom["S"], geom["m_k"], geom["kml"]
+    # units per launch: one launch covers all S macro segments of one query (or, for the
+    # statistics, all segments shared by the batch).  Per segment the LB_IP path must read
+    # its m_k target points once (8 B each: the target plus the m-1 halo) -- 8*n*(1+(m-1)/kml)
+    # per query -- and write a survivor bitmask of kml/8 bytes.
+    bytes_per_launch = 8.0 * S * m_k + S * kml / 8.0
+    avg_s = ms / max(1, launches) / 1e3
+    achieved = bytes_per_launch / avg_s / 1e9
+    traffic = None
+    try:
+        with open(PROFILE_SUMMARY) as f:
+            tr = json.load(f)
+        traffic = tr.get(name, {}).get("bytes_per_launch")
+    except Exception:
+        pass
+    return {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
+            "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
+            "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": round(avg_s * 1e3, 4),
+            "peak_source": peaks["source"] + " (MEASURED_PEAKS.json hbm_gbs)" if peaks["source"] == "measured"
+            else "fallback 6.65 TB/s"}
+
+
+def geometry(n, m):
+    sel = 1
+    while sel < 8 * m:
+        sel *= 2
+    m_k = min(sel, n)
+    kml = m_k - m + 1
+    tsn = n - m + 1
+    forsize, tail = tsn // kml, tsn % kml
+    return {"m_k": m_k, "kml": kml, "forsize": forsize, "tail": tail, "S": forsize + (1 if tail else 0)}
+
+
+# ------------------------------------------------------------------ reference arm
+
+def ref_binary():
+    return os.path.join(ROOT, "oracle", "_ref", "fsmeld_ref")
+
+
+def run_ref(args, env):
+    p = subprocess.run([ref_binary()] + [str(a) for a in args], capture_output=True, text=True, env=env)
+    if p.returncode != 0:
+        raise RuntimeError(p.stderr.strip())
+    return p.stdout
+
+
+def parse_valid(out):
+    for line in out.splitlines():
+        if line.startswith("Total Valid Candidates: "):
+            return int(line.split(": ")[1])
+    raise RuntimeError("no candidate count in reference output")
+
+
+def reference_setup(tmp, target, queries, cutoffs, slice_points):
+    """Write sample slices and query files for the reference binary."""
+    env = dict(os.environ, FSMELD_QUIET_MATCHES="1", FSMELD_RESULTS_CSV=os.path.join(tmp, "ref.csv"))
+    files = {}
+    for metric, _ in METRICS:
+        qp = os.path.join(tmp, f"q_{metric}.txt")
+        np.savetxt(qp, queries[metric], fmt="%.17g")
+        files[metric] = qp
+    slices = []
+    nslices = max(1, len(target) // slice_points)
+    for i in range(nslices):
+        sp = os.path.join(tmp, f"slice_{i}.bin")
+        target[i * slice_points:(i + 1) * slice_points].astype("<f8").tofile(sp)
+        slices.append(sp)
+    return env, files, slices
+
+
+def reference_step(env, files, slices, cutoffs, procs, offset):
+    """`procs` concurrent reference processes, each one search over one sample slice."""
+    jobs = []
+    for i in range(procs):
+        metric, arg = METRICS[(offset + i) % len(METRICS)]
+        sp = slices[(offset + i) % len(slices)]
+        jobs.append((sp, metric, arg))
+    t0 = time.perf_counter()
+    ps = [subprocess.Popen([ref_binary(), "search", sp, files[mt], str(M), repr(cutoffs[mt]), mt, str(W), ag],
+                           stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, env=env)
+          for sp, mt, ag in [(a, b, str(c)) for a, b, c in jobs]]
+    total = 0
+    for p in ps:
+        out, err = p.communicate()
+        if p.returncode != 0:
+            raise RuntimeError(err.strip())
+        total += parse_valid(out)
+    return total, time.perf_counter() - t0
+
+
+def impl_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    if not os.path.exists(ref_binary()):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/fsmeld_ref was not built"}))
+        return 0
+    target, queries = make_workload(0)
+    slice_points = 1 << 17
+    cores = os.cpu_count() or 1
+    cutoffs = dict(CUTOFFS)
+    with tempfile.TemporaryDirectory() as tmp:
+        env, files, slices = reference_setup(tmp, target, queries, cutoffs, slice_points)
+        procs = max(1, min(cores, 5 * len(slices)))
+        for i in range(args.warmup):
+            reference_step(env, files, slices, cutoffs, procs, i * procs)
+        cand, secs = 0, 0.0
+        for i in range(args.steps):
+            c, s = reference_step(env, files, slices, cutoffs, procs, (args.warmup + i) * procs)
+            cand += c
+            secs += s
+    value = cand / secs
+    sample = (f"per step {procs} concurrent reference `search` processes (one per host thread), each over a "
+              f"2^17-point slice of the workload's target with one of the five queries and its k=50 cutoff")
+    line = {"impl": "reference", "metric": "candidates/s", "value": value, "unit": "candidates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": N_POINTS, "m": M, "w": W, "k": K_TOP, "queries_per_step": procs},
+            "cpu_baseline": {"value": value, "unit": "candidates/s", "cores": procs, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "candidates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def cpu_baseline_single(target, queries, cutoffs):
+    """The reference's CPU path, one core, five searches over a 2^21-point sample."""
+    if not os.path.exists(ref_binary()):
+        return None
+    with tempfile.TemporaryDirectory() as tmp:
+        env = dict(os.environ, FSMELD_QUIET_MATCHES="1", FSMELD_RESULTS_CSV=os.path.join(tmp, "ref.csv"))
+        sp = os.path.join(tmp, "sample.bin")
+        target[: 1 << 18].astype("<f8").tofile(sp)
+        cand, secs = 0, 0.0
+        for metric, arg in METRICS:
+            qp = os.path.join(tmp, f"q_{metric}.txt")
+            np.savetxt(qp, queries[metric], fmt="%.17g")
+            t0 = time.perf_counter()
+            out = run_ref(["search", sp, qp, M, repr(cutoffs[metric]), metric, W, arg], env)
+            secs += time.perf_counter() - t0
+            cand += parse_valid(out)
+    return {"value": cand / secs, "unit": "candidates/s", "cores": 1, "kind": "reference",
+            "sample": "the reference's `search` (its own sources + project FFT shim), single thread, the five "
+                      "queries with the workload's cutoffs over the first 2^18 points of the target"}
+
+
+# ------------------------------------------------------------------ our arm
+
+def impl_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from fsmeld_b200 import api
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    target, queries = make_workload(rank)
+    geom = geometry(len(target), M)
+    eng = api.Engine(target, device=local)
+    cutoffs = {}
+    for metric, arg in METRICS:
+        _idx, dist_k, _c = eng.cutoff(queries[metric], M, K_TOP, metric, W, arg)
+        cutoffs[metric] = float(dist_k[-1])
+    cutoffs_match = (rank != 0) or all(cutoffs[k] == CUTOFFS[k] for k in CUTOFFS)
+    batch = [dict(query=queries[mt], m=M, metric=mt, w=W, arg=ag, cutoff=cutoffs[mt]) for mt, ag in METRICS]
+
+    def step():
+        res = eng.batch("search", batch)
+        for r in res:
+            if r["status"] != 0:
+                raise RuntimeError(f"query failed: {r['status']}")
+        return res
+
+    for _ in range(args.warmup):
+        step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    eng.set_profiling(True)
+    launches0 = eng.launches
+    dev_ms = 0.0
+    cand = 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            res = step()
+            dev_ms += eng.last_call_ms
+            cand += sum(r["counters"]["valid"] for r in res)
+    torch.cuda.synchronize()
+    launches = eng.launches - launches0
+    stages = eng.stage_times()
+    eng.set_profiling(False)
+    t_local = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
+    c_local = torch.tensor([float(cand)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
+        dist.all_reduce(c_local, op=dist.ReduceOp.SUM)
+        dist.barrier()
+    t_max_ms = float(t_local.item())
+    cand_all = float(c_local.item())
+    value = cand_all / (t_max_ms / 1e3)
+
+    # end to end: target upload from pinned host memory, batch, result read-back, every step
+    pinned = torch.from_numpy(target).pin_memory()
+    e2e_secs = 0.0
+    e2e_cand = 0
+    d2h = 0
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2 = api.Engine(device_ptr=None, target=pinned.numpy(), device=local)
+        res = e2.batch("search", batch)
+        e2.close()
+        t1 = time.perf_counter()
+        if i >= args.warmup:
+            e2e_secs += t1 - t0
+            e2e_cand += sum(r["counters"]["valid"] for r in res)
+            d2h = sum(int(r["count"]) * 8 + 96 for r in res)
+    e2e_value = e2e_cand / e2e_secs * world
+    h2d = len(target) * 8 + sum(M * 8 for _ in METRICS)
+
+    if rank == 0:
+        peaks = load_peaks()
+        dominant = max(stages.items(), key=lambda kv: kv[1][0])
+        line = {
+            "metric": "candidates/s", "value": value, "unit": "candidates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded random walks with motifs, NaN spans and flat runs; stands in for the "
+                    "reference's recorded datasets)",
+            "config": {"workload": WORKLOAD, "n": N_POINTS, "m": M, "w": W, "k": K_TOP,
+                       "queries_per_step": len(METRICS), "parallelism": f"{world} GPU(s), one target partition each",
+                       "l2": "inputs larger than L2 (134 MB target per GPU)",
+                       "cutoffs": cutoffs, "cutoffs_match_workload_constants": cutoffs_match},
+            "queries_per_s": len(METRICS) * world / (t_max_ms / 1e3 / args.steps),
+            "roofline": roofline(stages, dominant, geom, peaks, len(METRICS)),
+            "stage_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in stages.items()},
+            "e2e": {"value": e2e_value, "unit": "candidates/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_single(target, queries, cutoffs)
+        print(json.dumps(line))
+    eng.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return impl_reference(args)
+    return impl_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

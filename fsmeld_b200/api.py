@@ -79,6 +79,10 @@ def lib():
             "fsmeld_strerror": (C.c_char_p, [C.c_int]),
             "fsmeld_set_workspace_limit": (C.c_int, [ctxp, C.c_int64]),
             "fsmeld_kernel_launches": (C.c_int64, [ctxp]),
+            "fsmeld_set_profiling": (C.c_int, [ctxp, C.c_int]),
+            "fsmeld_stage_times": (C.c_int, [ctxp, dp, ip, C.c_int]),
+            "fsmeld_stage_name": (C.c_char_p, [C.c_int]),
+            "fsmeld_last_call_ms": (C.c_double, [ctxp]),
             "fsmeld_search": (C.c_int, [ctxp, dp, C.c_int, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int64,
                                         C.c_int64, ip, C.c_int64, ip, C.POINTER(Counters), ip]),
             "fsmeld_cutoff": (C.c_int, [ctxp, dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int64,
@@ -103,12 +107,12 @@ def lib():
     return _lib
 
 
-def exported_symbols():
+def exported_symbols(header=None):
     """Names of the C ABI entry points declared in include/fsmeld_cuda.h."""
-    return ["fsmeld_open", "fsmeld_open_file", "fsmeld_open_device", "fsmeld_close", "fsmeld_target_length",
-            "fsmeld_last_error", "fsmeld_strerror", "fsmeld_set_workspace_limit", "fsmeld_kernel_launches",
-            "fsmeld_search", "fsmeld_cutoff", "fsmeld_exact", "fsmeld_batch", "fsmeld_inspect",
-            "fsmeld_search_file", "fsmeld_cutoff_file", "fsmeld_exact_file"]
+    import re
+    header = header or os.path.join(os.path.dirname(_PKG), "include", "fsmeld_cuda.h")
+    text = re.sub(r"/\*.*?\*/", "", open(header).read(), flags=re.S)
+    return sorted(set(re.findall(r"\b(fsmeld_[a-z_0-9]+)\s*\(", text)))
 
 
 def _check(status, ctx=None):
@@ -168,6 +172,20 @@ class Engine:
     @property
     def launches(self):
         return lib().fsmeld_kernel_launches(self._ctx)
+
+    @property
+    def last_call_ms(self):
+        """Device time (CUDA events on the engine's stream) of the last query call."""
+        return lib().fsmeld_last_call_ms(self._ctx)
+
+    def set_profiling(self, on=True):
+        _check(lib().fsmeld_set_profiling(self._ctx, int(on)), self._ctx)
+
+    def stage_times(self):
+        ms = np.zeros(16)
+        n = np.zeros(16, dtype=np.int64)
+        k = lib().fsmeld_stage_times(self._ctx, _dptr(ms), _iptr(n), 16)
+        return {lib().fsmeld_stage_name(i).decode(): (float(ms[i]), int(n[i])) for i in range(k)}
 
     def set_workspace_limit(self, nbytes):
         _check(lib().fsmeld_set_workspace_limit(self._ctx, int(nbytes)), self._ctx)

@@ -79,6 +79,60 @@ __device__ __forceinline__ bool lbip_exceeds(double bound, double cutoff, int me
     return true;
 }
 
+// Envelope of a z-normalised candidate window at point k (radius w, clipped to
+// the window [0, m)), from the raw target: x -> (x - mu) / sigma is monotone,
+// so min/max commute with it exactly.  tp, lraw, uraw point at the window start.
+__device__ __forceinline__ void cand_env(int k, int m, int w, const double* tp, const double* lraw,
+                                         const double* uraw, double mu, double sg, double* lo, double* up) {
+    double a, b;
+    if (k >= w && k <= m - 1 - w) {
+        a = lraw[k];
+        b = uraw[k];
+    } else {
+        const int s = k - w < 0 ? 0 : k - w, e = k + w > m - 1 ? m - 1 : k + w;
+        a = tp[s];
+        b = a;
+        for (int i = s + 1; i <= e; ++i) {
+            const double v = tp[i];
+            a = fmin(a, v);
+            b = fmax(b, v);
+        }
+    }
+    *lo = ddiv(dsub(a, mu), sg);
+    *up = ddiv(dsub(b, mu), sg);
+}
+
+// Q->T term of query point x (index k) against the candidate envelope: the
+// per-point term of src/glb.cpp:306-372; LCSS returns the match indicator.
+__device__ __forceinline__ double qt_term(int metric, double x, int k, int m, int w, const double* tp,
+                                          const double* lraw, const double* uraw, double mu, double sg,
+                                          double arg) {
+    double lo, up;
+    cand_env(k, m, w, tp, lraw, uraw, mu, sg, &lo, &up);
+    switch (metric) {
+        case DTW:
+            if (x < lo) return dsq(x, lo);
+            if (x > up) return dsq(x, up);
+            return 0.0;
+        case ERP:
+            if (x > up) { const double p = dsq(x, up), r = dsq(x, arg); return (p < r) ? p : r; }
+            if (x < lo) { const double p = dsq(x, lo), r = dsq(x, arg); return (p < r) ? p : r; }
+            return 0.0;
+        case EDR:
+            if (x > up) return (fabs(dsub(x, up)) <= arg) ? 0.0 : 1.0;
+            if (x < lo) return (fabs(dsub(x, lo)) <= arg) ? 0.0 : 1.0;
+            return 0.0;
+        case LCSS:
+            if (x < lo) return (dsub(lo, x) <= arg) ? 1.0 : 0.0;
+            if (x > up) return (dsub(x, up) <= arg) ? 1.0 : 0.0;
+            return 1.0;
+        default:
+            if (x > up) { const double p = fabs(dsub(x, up)); return (p < arg) ? p : arg; }
+            if (x < lo) { const double p = fabs(dsub(x, lo)); return (p < arg) ? p : arg; }
+            return 0.0;
+    }
+}
+
 // Per-query tables prepared on the host (query z-normalisation as
 // src/fsmeld.cpp:622-643, powers with the C library's pow as
 // src/find_t_lp.cpp:253 etc.).

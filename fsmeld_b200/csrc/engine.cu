@@ -182,11 +182,19 @@ struct fsmeld_ctx {
     int smem_optin = 227 * 1024;
     long long ws_limit = 0;
     long long launches = 0;
+    double last_ms = 0.0;
     std::string err;
     struct Buf { void* p = nullptr; size_t bytes = 0; };
     std::map<std::string, Buf> bufs;
     std::map<int, double2*> twiddles;
     std::map<const void*, int> smem_set;
+    // opt-in per-stage device timing (CUDA events around each launch)
+    bool prof = false;
+    struct ProfRec { int stage; cudaEvent_t a, b; };
+    std::vector<ProfRec> pending;
+    std::vector<cudaEvent_t> pool;
+    double stage_ms[8] = {0};
+    long long stage_n[8] = {0};
 };
 
 namespace fsm {
@@ -232,8 +240,44 @@ static int allow_smem(fsmeld_ctx* c, K kernel, size_t bytes) {
     return FSMELD_OK;
 }
 
+enum Stage { ST_STATS, ST_ENV, ST_THR, ST_LBIP, ST_GLB1, ST_GLB2, ST_DP, ST_SELECT, ST_N };
+static const char* kStageNames[ST_N] = {"k_mvmean", "k_envelope", "k_threshold", "k_lbip",
+                                        "k_glb_tq", "k_glb_qt", "k_dp", "k_select"};
+
+static cudaEvent_t prof_event(fsmeld_ctx* c) {
+    if (!c->pool.empty()) { cudaEvent_t e = c->pool.back(); c->pool.pop_back(); return e; }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+static void prof_begin(fsmeld_ctx* c, int stage) {
+    if (!c->prof) return;
+    fsmeld_ctx::ProfRec r{stage, prof_event(c), prof_event(c)};
+    cudaEventRecord(r.a, c->stream);
+    c->pending.push_back(r);
+}
+static void prof_end(fsmeld_ctx* c) {
+    if (!c->prof || c->pending.empty()) return;
+    cudaEventRecord(c->pending.back().b, c->stream);
+}
+static void prof_collect(fsmeld_ctx* c) {
+    if (c->pending.empty()) return;
+    cudaStreamSynchronize(c->stream);
+    for (auto& r : c->pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+            c->stage_ms[r.stage] += ms;
+            c->stage_n[r.stage] += 1;
+        }
+        c->pool.push_back(r.a);
+        c->pool.push_back(r.b);
+    }
+    c->pending.clear();
+}
+
 #define LAUNCH_CHECK(c)                                                  \
     do {                                                                 \
+        prof_end(c);                                                     \
         (c)->launches++;                                                 \
         cudaError_t _le = cudaGetLastError();                            \
         if (_le != cudaSuccess) return cuda_fail(_le, "kernel launch", __FILE__, __LINE__); \
@@ -294,6 +338,8 @@ struct Stats {
     double* SIG = nullptr;
     double* Un = nullptr;
     double* Ln = nullptr;
+    double* Lraw = nullptr;  // centred radius-w min / max of the raw target
+    double* Uraw = nullptr;
 };
 
 static int run_stats(fsmeld_ctx* c, const Geom& g, Stats* st, const std::string& tag) {
@@ -303,6 +349,7 @@ static int run_stats(fsmeld_ctx* c, const Geom& g, Stats* st, const std::string&
     const size_t smem = mvmean_smem_bytes();
     if ((r = allow_smem(c, k_mvmean, smem))) return r;
     const unsigned blocks = (unsigned)((g.S + 31) / 32);
+    prof_begin(c, ST_STATS);
     k_mvmean<<<blocks, 32, smem, c->stream>>>(c->d_target, g, st->MU, st->SIG);
     LAUNCH_CHECK(c);
     return FSMELD_OK;
@@ -325,6 +372,7 @@ static int launch_env(fsmeld_ctx* c, const Geom& g, int w, Stats* st) {
         grid = (unsigned)std::min<long long>(g.S, (long long)c->sm_count * 2);
         if ((r = bufT(c, "envwork", (work / 8 + 1) * grid, &gwork))) return r;
     }
+    prof_begin(c, ST_ENV);
     k_envelope<T, OPT><<<grid, T, smem, c->stream>>>(c->d_target, st->MU, st->SIG, g, w, st->Un, st->Ln,
                                                      gwork, (long long)(work / 8 + 1));
     LAUNCH_CHECK(c);
@@ -335,6 +383,12 @@ static int run_env(fsmeld_ctx* c, const Geom& g, int w, Stats* st, const std::st
     int r;
     if ((r = bufT(c, "un" + tag, (size_t)g.S * g.m_k, &st->Un))) return r;
     if ((r = bufT(c, "ln" + tag, (size_t)g.S * g.m_k, &st->Ln))) return r;
+    if ((r = bufT(c, "lraw" + tag, (size_t)g.n, &st->Lraw))) return r;
+    if ((r = bufT(c, "uraw" + tag, (size_t)g.n, &st->Uraw))) return r;
+    prof_begin(c, ST_ENV);
+    k_raw_env<<<(unsigned)std::min<long long>((g.n + 255) / 256, (long long)c->sm_count * 32), 256, 0, c->stream>>>(
+        c->d_target, g.n, w, st->Lraw, st->Uraw);
+    LAUNCH_CHECK(c);
     const int mk = g.m_k;
     if (mk <= 1024) return launch_env<128, 8>(c, g, w, st);
     if (mk <= 2048) return launch_env<256, 8>(c, g, w, st);
@@ -362,6 +416,7 @@ static int launch_thr(fsmeld_ctx* c, const Geom& g, const ThrJob* djobs, int njo
         if ((r = bufT(c, "thrwork", work * gx * (size_t)njobs, &gwork))) return r;
     }
     dim3 grid(gx, njobs);
+    prof_begin(c, ST_THR);
     k_threshold<T, IPT><<<grid, T, smem, c->stream>>>(g, djobs, gwork, (long long)work);
     LAUNCH_CHECK(c);
     return FSMELD_OK;
@@ -411,16 +466,18 @@ static int run_lbip(fsmeld_ctx* c, const Geom& g, LbJob job) {
         job.slot_stride = (long long)smem;
         smem = 0;
     }
+    prof_begin(c, ST_LBIP);
     k_lbip<256><<<grid, 256, smem, c->stream>>>(g, job, W, P, logP);
     LAUNCH_CHECK(c);
     return FSMELD_OK;
 }
 
 // counters slot layout
-enum { C_SURV, C_G1, C_G2, C_OUT, C_VALID, C_SEED, C_SEEDOUT, C_N };
+enum { C_SURV, C_G1, C_G2, C_OUT, C_VALID, C_SEED, C_SEEDOUT, C_DPNEXT, C_N };
 
 static int run_glb(fsmeld_ctx* c, const Geom& g, const QueryDev& qd, const Stats& st, const long long* in,
-                   unsigned long long* cnt, long long cap, long long* segc, long long** out_list) {
+                   unsigned long long* cnt, long long cap, long long* segc, long long** out_list,
+                   double** out_qt = nullptr) {
     long long *g1, *g2;
     double *g1b, *g1t;
     int r;
@@ -430,22 +487,28 @@ static int run_glb(fsmeld_ctx* c, const Geom& g, const QueryDev& qd, const Stats
     if ((r = bufT(c, "g2", (size_t)cap, &g2))) return r;
     GlbJob j1{};
     j1.q = qd; j1.target = c->d_target; j1.MU = st.MU; j1.SIG = st.SIG;
+    j1.lraw = st.Lraw; j1.uraw = st.Uraw;
     j1.in = in; j1.n_in = cnt + C_SURV; j1.in_cap = cap;
     j1.out = g1; j1.out_b = g1b; j1.out_t = g1t; j1.n_out = cnt + C_G1; j1.out_cap = cap;
     j1.segc = segc;
     const size_t sm1 = sizeof(double) * 3 * qd.m;
     if ((r = allow_smem(c, k_glb_tq, sm1))) return r;
+    prof_begin(c, ST_GLB1);
     k_glb_tq<<<c->sm_count * 8, 256, sm1, c->stream>>>(g, j1);
     LAUNCH_CHECK(c);
     GlbJob j2 = j1;
+    double* g2t;
+    if ((r = bufT(c, "g2t", (size_t)cap, &g2t))) return r;
     j2.in = g1; j2.in_b = g1b; j2.in_t = g1t; j2.n_in = cnt + C_G1;
-    j2.out = g2; j2.out_b = nullptr; j2.out_t = nullptr; j2.n_out = cnt + C_G2;
-    int warps = 8;
-    while (warps > 1 && sizeof(double) * (size_t)qd.m * (1 + 2 * warps) > (size_t)c->smem_optin - 4096) warps >>= 1;
-    const size_t sm2 = sizeof(double) * (size_t)qd.m * (1 + 2 * warps);
+    j2.out = g2; j2.out_b = nullptr; j2.out_t = g2t; j2.n_out = cnt + C_G2;
+    const size_t sm2 = sizeof(double) * (((size_t)qd.m + 1) & ~(size_t)1);
     if ((r = allow_smem(c, k_glb_qt, sm2))) return r;
-    k_glb_qt<<<c->sm_count * 4, warps * 32, sm2, c->stream>>>(g, j2);
+    int per_sm = 0;
+    FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_glb_qt, 128, sm2));
+    prof_begin(c, ST_GLB2);
+    k_glb_qt<<<(unsigned)(std::max(1, per_sm) * c->sm_count), 128, sm2, c->stream>>>(g, j2);
     LAUNCH_CHECK(c);
+    if (out_qt) *out_qt = g2t;
     *out_list = g2;
     return FSMELD_OK;
 }
@@ -455,23 +518,44 @@ static int run_dp(fsmeld_ctx* c, const Geom& g, DpJob job, long long expected) {
     const int warps = 4;
     const size_t per_warp = dp_warp_doubles(w);
     size_t smem = sizeof(double) * (((size_t)job.q.m + 1) & ~(size_t)1) + sizeof(double) * per_warp * warps;
-    unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>((expected + warps * 32 - 1) / (warps * 32),
-                                                                        (long long)c->sm_count * 16));
     int r;
+    unsigned long long* next;
+    if ((r = bufT(c, "dpnext", 1, &next))) return r;
+    FSM_CUDA_TRY(cudaMemsetAsync(next, 0, sizeof(unsigned long long), c->stream));
+    job.next = next;
     job.gwork = nullptr;
+    const void* kf = job.q.metric == DTW ? (const void*)k_dp<DTW>
+                   : job.q.metric == ERP ? (const void*)k_dp<ERP>
+                   : job.q.metric == EDR ? (const void*)k_dp<EDR>
+                   : job.q.metric == LCSS ? (const void*)k_dp<LCSS> : (const void*)k_dp<MSM>;
+    unsigned grid;
     if (smem > (size_t)c->smem_optin - 4096) {
-        grid = (unsigned)std::min<long long>(grid, (long long)c->sm_count * 4);
+        grid = (unsigned)c->sm_count * 2;
         double* gw;
         if ((r = bufT(c, "dpwork", per_warp * warps * grid, &gw))) return r;
         job.gwork = gw;
         smem = sizeof(double) * (((size_t)job.q.m + 1) & ~(size_t)1);
     }
     switch (job.q.metric) {
-        case DTW: if ((r = allow_smem(c, k_dp<DTW>, smem))) return r; k_dp<DTW><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
-        case ERP: if ((r = allow_smem(c, k_dp<ERP>, smem))) return r; k_dp<ERP><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
-        case EDR: if ((r = allow_smem(c, k_dp<EDR>, smem))) return r; k_dp<EDR><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
-        case LCSS: if ((r = allow_smem(c, k_dp<LCSS>, smem))) return r; k_dp<LCSS><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
-        default: if ((r = allow_smem(c, k_dp<MSM>, smem))) return r; k_dp<MSM><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
+        case DTW: if ((r = allow_smem(c, k_dp<DTW>, smem))) return r; break;
+        case ERP: if ((r = allow_smem(c, k_dp<ERP>, smem))) return r; break;
+        case EDR: if ((r = allow_smem(c, k_dp<EDR>, smem))) return r; break;
+        case LCSS: if ((r = allow_smem(c, k_dp<LCSS>, smem))) return r; break;
+        default: if ((r = allow_smem(c, k_dp<MSM>, smem))) return r; break;
+    }
+    if (!job.gwork) {
+        int per_sm = 0;
+        FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf, warps * 32, smem));
+        const long long want = (expected + warps * 32 - 1) / (warps * 32);
+        grid = (unsigned)std::max<long long>(1, std::min<long long>(want, (long long)std::max(1, per_sm) * c->sm_count));
+    }
+    prof_begin(c, ST_DP);
+    switch (job.q.metric) {
+        case DTW: k_dp<DTW><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
+        case ERP: k_dp<ERP><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
+        case EDR: k_dp<EDR><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
+        case LCSS: k_dp<LCSS><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
+        default: k_dp<MSM><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
     }
     LAUNCH_CHECK(c);
     return FSMELD_OK;
@@ -600,14 +684,16 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
         lj.nvalid = cnt + C_VALID; lj.segc = segc;
         if ((r = run_lbip(c, g, lj))) return r;
         long long* g2;
-        if ((r = run_glb(c, g, qd, st, surv, cnt, cap, segc, &g2))) return r;
+        double* g2t;
+        if ((r = run_glb(c, g, qd, st, surv, cnt, cap, segc, &g2, &g2t))) return r;
         long long* oi;
         double* od;
         if ((r = bufT(c, "outi", (size_t)cap, &oi))) return r;
         if ((r = bufT(c, "outd", (size_t)cap, &od))) return r;
         DpJob dj{};
         dj.q = qd; dj.target = c->d_target; dj.MU = st.MU; dj.SIG = st.SIG;
-        dj.list = g2; dj.n_list = cnt + C_G2; dj.list_cap = cap; dj.mode = 0; dj.cutoff = qr.cutoff;
+        dj.lraw = st.Lraw; dj.uraw = st.Uraw;
+        dj.list = g2; dj.list_s = g2t; dj.n_list = cnt + C_G2; dj.list_cap = cap; dj.mode = 0; dj.cutoff = qr.cutoff;
         dj.out_idx = oi; dj.out_dist = od; dj.n_out = cnt + C_OUT; dj.out_cap = cap; dj.n_valid = nullptr;
         if ((r = run_dp(c, g, dj, (long long)c->sm_count * 16 * 128))) return r;
         FSM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
@@ -643,6 +729,7 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
     // seeds
     long long* seeds;
     if ((r = bufT(c, "seeds", (size_t)g.S, &seeds))) return r;
+    prof_begin(c, ST_SELECT);
     k_seed<<<(unsigned)std::min<long long>(g.S, (long long)c->sm_count * 8), 256, 0, c->stream>>>(
         g, z, st.SIG, 1, seeds, cnt + C_SEED, g.S);
     LAUNCH_CHECK(c);
@@ -652,7 +739,7 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
     if ((r = bufT(c, "seedd", (size_t)g.S, &sd))) return r;
     DpJob sj{};
     sj.q = qd; sj.target = c->d_target; sj.MU = st.MU; sj.SIG = st.SIG;
-    sj.list = seeds; sj.n_list = cnt + C_SEED; sj.list_cap = g.S; sj.mode = 1; sj.cutoff = 0.0;
+    sj.list = seeds; sj.n_list = cnt + C_SEED; sj.list_cap = g.S; sj.mode = 1; sj.cutoff = DBL_MAX;
     sj.out_idx = si; sj.out_dist = sd; sj.n_out = cnt + C_SEEDOUT; sj.out_cap = g.S;
     if ((r = run_dp(c, g, sj, g.S))) return r;
     FSM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
@@ -670,20 +757,23 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
     // filter, GLB and DP at tau
     long long* f1;
     if ((r = bufT(c, "surv", (size_t)cap, &f1))) return r;
+    prof_begin(c, ST_SELECT);
     k_lb_filter<<<(unsigned)std::min<long long>((g.tsn + 255) / 256, (long long)c->sm_count * 16), 256, 0, c->stream>>>(
         g, z, st.SIG, tau, qd.metric, f1, cnt + C_SURV, cap);
     LAUNCH_CHECK(c);
     QueryDev qt = qd;
     qt.cutoff = tau;
     long long* g2;
-    if ((r = run_glb(c, g, qt, st, f1, cnt, cap, nullptr, &g2))) return r;
+    double* g2t;
+    if ((r = run_glb(c, g, qt, st, f1, cnt, cap, nullptr, &g2, &g2t))) return r;
     long long* oi;
     double* od;
     if ((r = bufT(c, "outi", (size_t)cap, &oi))) return r;
     if ((r = bufT(c, "outd", (size_t)cap, &od))) return r;
     DpJob dj{};
     dj.q = qt; dj.target = c->d_target; dj.MU = st.MU; dj.SIG = st.SIG;
-    dj.list = g2; dj.n_list = cnt + C_G2; dj.list_cap = cap; dj.mode = 1; dj.cutoff = tau;
+    dj.lraw = st.Lraw; dj.uraw = st.Uraw;
+    dj.list = g2; dj.list_s = g2t; dj.n_list = cnt + C_G2; dj.list_cap = cap; dj.mode = 1; dj.cutoff = tau;
     dj.out_idx = oi; dj.out_dist = od; dj.n_out = cnt + C_OUT; dj.out_cap = cap;
     if ((r = run_dp(c, g, dj, (long long)c->sm_count * 16 * 128))) return r;
     FSM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
@@ -822,6 +912,8 @@ int fsmeld_close(fsmeld_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (auto& kv : c->bufs) if (kv.second.p) cudaFree(kv.second.p);
     for (auto& kv : c->twiddles) cudaFree(kv.second);
+    for (auto& r : c->pending) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (auto e : c->pool) cudaEventDestroy(e);
     if (c->own_target && c->d_target) cudaFree(c->d_target);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -859,6 +951,28 @@ int fsmeld_set_workspace_limit(fsmeld_ctx* c, int64_t bytes) {
 
 int64_t fsmeld_kernel_launches(const fsmeld_ctx* c) { return c ? c->launches : 0; }
 
+double fsmeld_last_call_ms(const fsmeld_ctx* c) { return c ? c->last_ms : 0.0; }
+
+int fsmeld_set_profiling(fsmeld_ctx* c, int on) {
+    if (!c) return FSMELD_E_ARG;
+    prof_collect(c);
+    c->prof = on != 0;
+    for (int i = 0; i < ST_N; ++i) { c->stage_ms[i] = 0; c->stage_n[i] = 0; }
+    return FSMELD_OK;
+}
+
+int fsmeld_stage_times(fsmeld_ctx* c, double* ms, int64_t* launches, int cap) {
+    if (!c) return FSMELD_E_ARG;
+    prof_collect(c);
+    for (int i = 0; i < ST_N && i < cap; ++i) {
+        if (ms) ms[i] = c->stage_ms[i];
+        if (launches) launches[i] = c->stage_n[i];
+    }
+    return ST_N;
+}
+
+const char* fsmeld_stage_name(int i) { return (i >= 0 && i < ST_N) ? kStageNames[i] : ""; }
+
 static int single(fsmeld_ctx* c, int mode, const double* query, int m, double cutoff, int k, int metric,
                   int w, double arg, int64_t eb, int64_t ee, int64_t* out_idx, double* out_dist,
                   int64_t cap, int64_t* out_count, fsmeld_counters* counters, int64_t* seg_counts) {
@@ -881,8 +995,10 @@ static int single(fsmeld_ctx* c, int mode, const double* query, int m, double cu
     r = run_batch(c, runs, &st);
     cudaEventRecord(c->ev1, c->stream);
     cudaEventSynchronize(c->ev1);
+    prof_collect(c);
     float ms = 0;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->last_ms = ms;
     if (counters) counters->device_ms = ms;
     return r;
 }
@@ -932,7 +1048,14 @@ int fsmeld_batch(fsmeld_ctx* c, int mode, const fsmeld_query* qs, int nq, fsmeld
     int r = run_batch(c, runs, &st);
     cudaEventRecord(c->ev1, c->stream);
     cudaEventSynchronize(c->ev1);
-    for (size_t j = 0; j < map.size(); ++j) res[map[j]].status = st[j];
+    prof_collect(c);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->last_ms = ms;
+    for (size_t j = 0; j < map.size(); ++j) {
+        res[map[j]].status = st[j];
+        res[map[j]].counters.device_ms = ms;
+    }
     int first = r;
     for (int i = 0; i < nq && !first; ++i) first = res[i].status;
     return first;

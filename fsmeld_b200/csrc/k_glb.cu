@@ -4,10 +4,14 @@
 //    T->Q sum with early abandon, z-normalising candidate points lazily
 //    (t - mu) / sigma exactly as src/fsmeld.cpp:823-826 does, so abandoned
 //    candidates never pay for the whole window;
-//  * k_glb_qt: one warp per T->Q survivor builds the candidate envelope
-//    (radius w, no NaN possible in a valid window) and the Q->T terms in
-//    parallel; lane 0 adds the terms in the reference's order, so the bound
-//    carries the reference's bits.
+//  * k_glb_qt: one lane per T->Q survivor adds the Q->T terms in the
+//    reference's order.  The candidate envelope (lower_upper_lemire of the
+//    z-normalised window, src/glb.cpp:302-304) is never materialised:
+//    z-normalisation x -> (x - mu) / sigma is monotone even after rounding,
+//    so the minimum of the normalised points equals the normalised minimum of
+//    the raw points, bit for bit; interior envelope points come from a
+//    precomputed raw envelope of the target (k_raw_env) and only the 2w
+//    clipped edge windows are scanned.
 // Early abandon compares a running sum of non-negative terms with the
 // cutoff; running sums never decrease, so testing the final sum once is the
 // same decision as testing after every term.
@@ -152,15 +156,30 @@ __global__ void __launch_bounds__(256) k_glb_tq(Geom g, GlbJob job) {
     }
 }
 
-// one warp per T->Q survivor
-__global__ void __launch_bounds__(256) k_glb_qt(Geom g, GlbJob job) {
+// Centred radius-w min/max of the raw target (NaN ignored; only positions
+// inside valid windows are ever read back).
+__global__ void __launch_bounds__(256) k_raw_env(const double* __restrict__ t, long long n, int w,
+                                                 double* __restrict__ lo, double* __restrict__ up) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (long long)gridDim.x * blockDim.x) {
+        const long long a = p - w < 0 ? 0 : p - w, b = p + w > n - 1 ? n - 1 : p + w;
+        double mn = t[a], mx = t[a];
+        for (long long i = a + 1; i <= b; ++i) {
+            const double v = t[i];
+            mn = fmin(mn, v);
+            mx = fmax(mx, v);
+        }
+        lo[p] = mn;
+        up[p] = mx;
+    }
+}
+
+// one lane per T->Q survivor: Q->T terms added in the reference's order
+__global__ void __launch_bounds__(128) k_glb_qt(Geom g, GlbJob job) {
     extern __shared__ double gqt_smem[];
     const QueryDev& q = job.q;
     const int m = q.m, metric = q.metric, w = q.w;
-    const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double* Q = gqt_smem;
-    double* Tw = Q + m + warp * 2 * m;   // normalised candidate
-    double* term = Tw + m;               // Q->T terms
     for (int i = threadIdx.x; i < m; i += blockDim.x) Q[i] = q.qn[i];
     __syncthreads();
     const double bsf = q.cutoff;
@@ -168,81 +187,39 @@ __global__ void __launch_bounds__(256) k_glb_qt(Geom g, GlbJob job) {
     const double arg = q.arg;
     const unsigned long long n_in = *job.n_in;
     const unsigned long long n_lim = n_in < (unsigned long long)job.in_cap ? n_in : job.in_cap;
-    for (unsigned long long c = (unsigned long long)blockIdx.x * warps + warp; c < n_lim;
-         c += (unsigned long long)gridDim.x * warps) {
+    for (unsigned long long c = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; c < n_lim;
+         c += (unsigned long long)gridDim.x * blockDim.x) {
         const long long gi = job.in[c];
         const double boundary = job.in_b[c];
         const double tq = job.in_t[c];
         long long s;
         int j;
         g.locate(gi, &s, &j);
-        double glb;
+        double glb, qt = 0.0;
         if (boundary == -1.0) {
             glb = kGlbMax;  // abandoned in T->Q but MAX_VAL <= cutoff
         } else {
             const double mu = job.MU[s * g.kml + j], sg = job.SIG[s * g.kml + j];
-            const double* tp = job.target + gi;
-            for (int k = lane; k < m; k += 32) Tw[k] = ddiv(dsub(tp[k], mu), sg);
-            __syncwarp();
-            // candidate envelope (src/glb.cpp:302-304 -> src/lower_upper_lemire.cpp:8-44)
-            double qr = 0.0;
-            for (int k = lane; k < m; k += 32) {
-                const int a = max(0, k - w), b = min(m - 1, k + w);
-                double lo = Tw[a], hi = Tw[a];
-                for (int i = a + 1; i <= b; ++i) {
-                    const double v = Tw[i];
-                    lo = (v <= lo) ? v : lo;
-                    hi = (v >= hi) ? v : hi;
-                }
-                const double x = Q[k];
-                double tm = 0.0;
-                switch (metric) {
-                    case DTW:
-                        if (x < lo) tm = dsq(x, lo);
-                        else if (x > hi) tm = dsq(x, hi);
-                        break;
-                    case ERP:
-                        if (x > hi) tm = dminv(dsq(x, hi), dsq(x, arg));
-                        else if (x < lo) tm = dminv(dsq(x, lo), dsq(x, arg));
-                        break;
-                    case EDR:
-                        if (x > hi) tm = edr_sub(x, hi, arg);
-                        else if (x < lo) tm = edr_sub(x, lo, arg);
-                        break;
-                    case LCSS:
-                        tm = env_match(x, lo, hi, arg) ? 1.0 : 0.0;
-                        break;
-                    default:
-                        if (x > hi) tm = dminv(fabs(dsub(x, hi)), arg);
-                        else if (x < lo) tm = dminv(fabs(dsub(x, lo)), arg);
-                        break;
-                }
-                term[k] = tm;
-                if (metric == LCSS) qr += tm;
-            }
-            __syncwarp();
+            const int k0 = (metric == LCSS) ? 0 : 1, k1 = (metric == LCSS) ? m - 1 : m - 2;
+            for (int k = k0; k <= k1; ++k)
+                qt = dadd(qt, qt_term(metric, Q[k], k, m, w, job.target + gi, job.lraw + gi, job.uraw + gi, mu,
+                                      sg, arg));
             if (metric == LCSS) {
-                for (int o = 16; o; o >>= 1) qr += __shfl_xor_sync(0xffffffffu, qr, o);
-                const double min_len = (double)m;
-                glb = dmax0(dsub(1.0, ddiv(dminv(tq, qr), min_len)));
+                glb = dmax0(dsub(1.0, ddiv(dminv(tq, qt), (double)m)));
             } else {
-                double qt = 0.0;
-                if (lane == 0)
-                    for (int k = 1; k < m - 1; ++k) qt = dadd(qt, term[k]);
-                qt = __shfl_sync(0xffffffffu, qt, 0);
                 const double tot = dadd(boundary, qt);
-                if (metric == DTW || metric == ERP) {
+                if (metric == DTW || metric == ERP)
                     glb = (tot > sq) ? kGlbMax : dsqrt(dmax0(dadd(boundary, dmaxv(tq, qt))));
-                } else {
+                else
                     glb = (tot > bsf) ? kGlbMax : dadd(boundary, dmaxv(tq, qt));
-                }
             }
-            __syncwarp();
         }
-        const bool keep = glb <= bsf;
-        if (lane == 0 && keep) {
+        if (glb <= bsf) {
             const unsigned long long o = atomicAdd(job.n_out, 1ull);
-            if (o < (unsigned long long)job.out_cap) job.out[o] = gi;
+            if (o < (unsigned long long)job.out_cap) {
+                job.out[o] = gi;
+                if (job.out_t) job.out_t[o] = (boundary == -1.0) ? -1.0 : qt;
+            }
             if (job.segc && s < g.forsize) atomicAdd((unsigned long long*)&job.segc[3 * s + 2], 1ull);
         }
     }

@@ -31,6 +31,8 @@ struct LbJob {
 struct GlbJob {
     QueryDev q;
     const double* target;
+    const double* lraw;         // centred radius-w min / max of the raw target
+    const double* uraw;
     const double* MU;
     const double* SIG;
     const long long* in;
@@ -49,9 +51,12 @@ struct GlbJob {
 struct DpJob {
     QueryDev q;
     const double* target;
+    const double* lraw;         // raw target envelope (cascading abandon terms)
+    const double* uraw;
     const double* MU;
     const double* SIG;
     const long long* list;      // candidates, or null for windows [0, n_windows)
+    const double* list_s;       // optional: GLB Q->T sum per candidate (cascading abandon)
     const unsigned long long* n_list;
     long long list_cap;
     long long n_windows;
@@ -62,6 +67,7 @@ struct DpJob {
     unsigned long long* n_out;
     long long out_cap;
     unsigned long long* n_valid;
+    unsigned long long* next;   // work counter (zeroed before the launch)
     double* gwork;              // global band scratch when shared memory is too small
 };
 
@@ -78,6 +84,8 @@ template <int T>
 __global__ void k_lbip(Geom g, LbJob job, const double2* __restrict__ W, int P, int logP);
 __global__ void k_glb_tq(Geom g, GlbJob job);
 __global__ void k_glb_qt(Geom g, GlbJob job);
+__global__ void k_raw_env(const double* __restrict__ t, long long n, int w, double* __restrict__ lo,
+                          double* __restrict__ up);
 template <int METRIC>
 __global__ void k_dp(Geom g, DpJob job);
 __global__ void k_lb_filter(Geom g, const double* __restrict__ z, const double* __restrict__ SIG,

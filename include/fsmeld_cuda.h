@@ -109,6 +109,16 @@ const char* fsmeld_strerror(int status);
 int fsmeld_set_workspace_limit(fsmeld_ctx* ctx, int64_t bytes);
 /* Number of CUDA kernel launches issued by this context so far. */
 int64_t fsmeld_kernel_launches(const fsmeld_ctx* ctx);
+/* Per-stage device timing (no counterpart in the reference): when on, each
+ * kernel launch is bracketed by CUDA events on the context's stream and its
+ * time is added to its stage; fsmeld_stage_times copies per-stage totals (ms)
+ * and launch counts and returns the number of stages; fsmeld_stage_name names
+ * stage i (the kernel). */
+int fsmeld_set_profiling(fsmeld_ctx* ctx, int on);
+int fsmeld_stage_times(fsmeld_ctx* ctx, double* ms, int64_t* launches, int cap);
+const char* fsmeld_stage_name(int stage);
+/* Device time (ms, CUDA events on the context's stream) of the last query call. */
+double fsmeld_last_call_ms(const fsmeld_ctx* ctx);
 
 /* ---- single queries (src/fsmeld.cpp:570-1074, 185-569, 1075-1344) --- */
 
