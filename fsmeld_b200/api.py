@@ -92,6 +92,9 @@ def lib():
             "fsmeld_batch": (C.c_int, [ctxp, C.c_int, C.POINTER(Query), C.c_int, C.POINTER(Result)]),
             "fsmeld_inspect": (C.c_int64, [ctxp, dp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, dp,
                                            C.c_int64]),
+            "fsmeld_exact_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_int64, dp, C.c_int, C.c_int, C.c_int,
+                                               C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_int64, ip,
+                                               C.c_void_p]),
             "fsmeld_search_file": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_double, C.c_char_p, C.c_int,
                                              C.c_double, C.c_int64, C.c_int64]),
             "fsmeld_cutoff_file": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_char_p, C.c_int,
@@ -279,6 +282,18 @@ def _kml(m, n):
         sel *= 2
     sel = min(sel, n)
     return sel - m + 1
+
+
+def exact_noalloc(device_target_ptr, n, query, m, cutoff, metric, w, arg, out_idx_ptr, out_dist_ptr, capacity,
+                  device=0, stream=None):
+    """fsmeld_exact_noalloc: device pointers in and out, no device allocation."""
+    q = np.ascontiguousarray(query[:m], dtype=np.float64)
+    count = C.c_int64(0)
+    st = lib().fsmeld_exact_noalloc(device, C.c_void_p(device_target_ptr), int(n), _dptr(q), m, _metric(metric), w,
+                                    float(arg), float(cutoff), C.c_void_p(out_idx_ptr), C.c_void_p(out_dist_ptr),
+                                    int(capacity), C.byref(count), C.c_void_p(stream) if stream else None)
+    _check(st)
+    return count.value
 
 
 # ---- reference-named entry points (print the reference's output) -------------

@@ -31,7 +31,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-static-global-template-stub=false",
                   "-Xcompiler", "-fPIC,-ffp-contract=off", f"-I{INCLUDE}"]
 
-CU = ["k_stats", "k_envelope", "k_threshold", "k_lbip", "k_glb", "k_dp", "k_select", "engine"]
+CU = ["k_stats", "k_envelope", "k_threshold", "k_lbip", "k_glb", "k_dp", "k_select", "engine", "noalloc"]
 
 
 def _newer(src_files, out):

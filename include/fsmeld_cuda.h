@@ -148,6 +148,28 @@ int fsmeld_batch(fsmeld_ctx* ctx, int mode, const fsmeld_query* queries, int nq,
 int64_t fsmeld_inspect(fsmeld_ctx* ctx, const double* query, int m, int metric, int w, double arg,
                        int what, double* out, int64_t cap);
 
+/* ---- exact scan that allocates no device memory (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc -- a serving loop
+ * whose device memory belongs to another allocator (a framework's caching
+ * pool, a memory-capped tenant) or code that must not allocate while a
+ * request is in flight.  Same results as fsmeld_exact without an exclusion
+ * interval: every valid window of device_target[0..n) through the banded
+ * elastic DP; matches (distance <= cutoff) written in ascending window order
+ * to the caller's device buffers device_out_idx / device_out_dist (at most
+ * capacity entries; *host_out_count gets the total); runs on `stream` (a
+ * cudaStream_t, NULL for the default stream) and returns after it finishes.
+ * Scratch is one static device array of 12 MiB per GPU, held until exit.
+ * Limits: n - m + 1 <= FSMELD_NOALLOC_MAX_WINDOWS, m <= FSMELD_NOALLOC_MAX_M,
+ * and the DP band (2w+1) must fit shared memory; larger requests return
+ * FSMELD_E_ARG with a message.  The first call on a device looks up the
+ * scratch array's device address: make it before any stream capture.  Calls
+ * share the array: calls that overlap on the GPU race, so serialise them. */
+#define FSMELD_NOALLOC_MAX_WINDOWS 262144
+#define FSMELD_NOALLOC_MAX_M 2048
+int fsmeld_exact_noalloc(int device, const double* device_target, int64_t n, const double* host_query, int m,
+                         int metric, int w, double arg, double cutoff, int64_t* device_out_idx,
+                         double* device_out_dist, int64_t capacity, int64_t* host_out_count, void* stream);
+
 /* ---- drop-ins for the reference's entry points (include/funcs.h:64-72):
  *      read TARGET.bin / QUERY.txt, print the reference's stdout lines and
  *      append the experiment CSV.  tag is "dtw", "erp", "edr", "lcss" or
