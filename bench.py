@@ -55,9 +55,9 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
-def make_workload(rank):
+def make_workload(rank, n_points=N_POINTS):
     from fsmeld_b200.synth import query_from, walk_with_structure
-    t = walk_with_structure(N_POINTS, M, seed=2 + 7919 * rank)
+    t = walk_with_structure(n_points, M, seed=2 + 7919 * rank)
     rng = np.random.default_rng(1002 + rank)
     queries = {}
     for metric, _ in METRICS:
@@ -298,15 +298,20 @@ def impl_ours(args):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
-    target, queries = make_workload(rank)
+    target, queries = make_workload(rank, args.n_points)
     geom = geometry(len(target), M)
     eng = api.Engine(target, device=local)
-    cutoffs = {}
-    for metric, arg in METRICS:
-        _idx, dist_k, _c = eng.cutoff(queries[metric], M, K_TOP, metric, W, arg)
-        cutoffs[metric] = float(dist_k[-1])
-    cutoffs_match = (rank != 0) or all(cutoffs[k] == CUTOFFS[k] for k in CUTOFFS)
-    batch = [dict(query=queries[mt], m=M, metric=mt, w=W, arg=ag, cutoff=cutoffs[mt]) for mt, ag in METRICS]
+    metrics = [(mt, ag) for mt, ag in METRICS if args.case in (None, mt)]
+    if args.case or args.n_points != N_POINTS:
+        cutoffs = dict(CUTOFFS)  # profiling cases: the workload's constants, no setup launches
+        cutoffs_match = None
+    else:
+        cutoffs = {}
+        for metric, arg in METRICS:
+            _idx, dist_k, _c = eng.cutoff(queries[metric], M, K_TOP, metric, W, arg)
+            cutoffs[metric] = float(dist_k[-1])
+        cutoffs_match = (rank != 0) or all(cutoffs[k] == CUTOFFS[k] for k in CUTOFFS)
+    batch = [dict(query=queries[mt], m=M, metric=mt, w=W, arg=ag, cutoff=cutoffs[mt]) for mt, ag in metrics]
 
     def step():
         res = eng.batch("search", batch)
@@ -343,23 +348,25 @@ def impl_ours(args):
     cand_all = float(c_local.item())
     value = cand_all / (t_max_ms / 1e3)
 
-    # end to end: target upload from pinned host memory, batch, result read-back, every step
+    # end to end through the public API: every step uploads the target from pinned host
+    # memory into the engine (fsmeld_load) and runs the batch, whose results come back to
+    # host memory
     pinned = torch.from_numpy(target).pin_memory()
+    pinned_np = pinned.numpy()
     e2e_secs = 0.0
     e2e_cand = 0
     d2h = 0
-    for i in range(args.warmup + args.steps):
+    for i in range(0 if args.no_e2e else args.warmup + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        e2 = api.Engine(device_ptr=None, target=pinned.numpy(), device=local)
-        res = e2.batch("search", batch)
-        e2.close()
+        eng.load(pinned_np)
+        res = eng.batch("search", batch)
         t1 = time.perf_counter()
         if i >= args.warmup:
             e2e_secs += t1 - t0
             e2e_cand += sum(r["counters"]["valid"] for r in res)
             d2h = sum(int(r["count"]) * 8 + 96 for r in res)
-    e2e_value = e2e_cand / e2e_secs * world
+    e2e_value = e2e_cand / e2e_secs * world if e2e_secs > 0 else None
     h2d = len(target) * 8 + sum(M * 8 for _ in METRICS)
 
     if rank == 0:
@@ -371,19 +378,20 @@ def impl_ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded random walks with motifs, NaN spans and flat runs; stands in for the "
                     "reference's recorded datasets)",
-            "config": {"workload": WORKLOAD, "n": N_POINTS, "m": M, "w": W, "k": K_TOP,
-                       "queries_per_step": len(METRICS), "parallelism": f"{world} GPU(s), one target partition each",
+            "config": {"workload": WORKLOAD if not args.case else f"{args.case} query of: {WORKLOAD}",
+                       "n": args.n_points, "m": M, "w": W, "k": K_TOP,
+                       "queries_per_step": len(metrics), "parallelism": f"{world} GPU(s), one target partition each",
                        "l2": "inputs larger than L2 (134 MB target per GPU)",
                        "cutoffs": cutoffs, "cutoffs_match_workload_constants": cutoffs_match},
-            "queries_per_s": len(METRICS) * world / (t_max_ms / 1e3 / args.steps),
-            "roofline": roofline(stages, dominant, geom, peaks, len(METRICS)),
+            "queries_per_s": len(metrics) * world / (t_max_ms / 1e3 / args.steps),
+            "roofline": roofline(stages, dominant, geom, peaks, len(metrics)),
             "stage_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in stages.items()},
             "e2e": {"value": e2e_value, "unit": "candidates/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
-        if world == 1 and not args.no_cpu_baseline:
+        if world == 1 and not args.no_cpu_baseline and not args.case and args.n_points == N_POINTS:
             line["cpu_baseline"] = cpu_baseline_single(target, queries, cutoffs)
         print(json.dumps(line))
     eng.close()
@@ -400,6 +408,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--case", choices=[m for m, _ in METRICS], help="one metric's query only (profiling runs)")
+    ap.add_argument("--n-points", type=int, default=N_POINTS, help="target length (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         return impl_reference(args)

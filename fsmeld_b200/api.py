@@ -72,6 +72,7 @@ def lib():
         sig = {
             "fsmeld_open": (C.c_int, [C.c_int, dp, C.c_int64, C.POINTER(ctxp)]),
             "fsmeld_open_file": (C.c_int, [C.c_int, C.c_char_p, C.POINTER(ctxp)]),
+            "fsmeld_load": (C.c_int, [ctxp, dp, C.c_int64]),
             "fsmeld_open_device": (C.c_int, [C.c_int, C.c_void_p, C.c_int64, C.POINTER(ctxp)]),
             "fsmeld_close": (C.c_int, [ctxp]),
             "fsmeld_target_length": (C.c_int64, [ctxp]),
@@ -154,6 +155,12 @@ class Engine:
             t = np.ascontiguousarray(target, dtype=np.float64)
             _check(L.fsmeld_open(device, _dptr(t), len(t), C.byref(self._ctx)))
         self.n = L.fsmeld_target_length(self._ctx)
+
+    def load(self, target):
+        """Replace the target (host array, e.g. pinned memory) keeping the workspace."""
+        t = np.ascontiguousarray(target, dtype=np.float64)
+        _check(lib().fsmeld_load(self._ctx, _dptr(t), len(t)), self._ctx)
+        self.n = len(t)
 
     def close(self):
         if self._ctx:

@@ -880,6 +880,22 @@ int fsmeld_open(int device, const double* host_target, int64_t n, fsmeld_ctx** o
     return FSMELD_OK;
 }
 
+int fsmeld_load(fsmeld_ctx* c, const double* host_target, int64_t n) {
+    if (!c || !host_target || n <= 0) return fail(FSMELD_E_ARG, "invalid target");
+    FSM_CUDA_TRY(cudaSetDevice(c->device));
+    if (!c->own_target || c->n < n) {
+        if (c->own_target && c->d_target) cudaFree(c->d_target);
+        c->d_target = nullptr;
+        c->own_target = false;
+        FSM_CUDA_TRY(cudaMalloc(&c->d_target, sizeof(double) * n));
+        c->own_target = true;
+    }
+    FSM_CUDA_TRY(cudaMemcpyAsync(c->d_target, host_target, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->n = n;
+    return FSMELD_OK;
+}
+
 int fsmeld_open_device(int device, const double* device_target, int64_t n, fsmeld_ctx** out) {
     if (!out || !device_target || n <= 0) return fail(FSMELD_E_ARG, "invalid target");
     fsmeld_ctx* c;

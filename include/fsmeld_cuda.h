@@ -99,6 +99,9 @@ typedef struct {
 int fsmeld_open(int device, const double* host_target, int64_t n, fsmeld_ctx** out);
 /* Read a target file (headerless doubles) into a new context. */
 int fsmeld_open_file(int device, const char* path, fsmeld_ctx** out);
+/* Replace the context's target with a host series (copied; the device buffer
+ * is reused when large enough). */
+int fsmeld_load(fsmeld_ctx* ctx, const double* host_target, int64_t n);
 /* Use a target already resident in device memory (not copied, not freed). */
 int fsmeld_open_device(int device, const double* device_target, int64_t n, fsmeld_ctx** out);
 int fsmeld_close(fsmeld_ctx* ctx);
