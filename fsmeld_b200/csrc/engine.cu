@@ -182,6 +182,9 @@ struct fsmeld_ctx {
     int smem_optin = 227 * 1024;
     long long ws_limit = 0;
     long long launches = 0;
+    // FSMELD_DP_EXACT=1: run every DP candidate in the exact boundary mode
+    // (same results; a diagnostic switch for the mode that in-range data never needs)
+    bool dp_exact = false;
     double last_ms = 0.0;
     std::string err;
     struct Buf { void* p = nullptr; size_t bytes = 0; };
@@ -515,26 +518,29 @@ static int run_glb(fsmeld_ctx* c, const Geom& g, const QueryDev& qd, const Stats
 
 static int run_dp(fsmeld_ctx* c, const Geom& g, DpJob job, long long expected) {
     const int w = job.q.w;
-    const int warps = 4;
+    const int warps = kDpThreads / 32;
     const size_t per_warp = dp_warp_doubles(w);
-    size_t smem = sizeof(double) * (((size_t)job.q.m + 1) & ~(size_t)1) + sizeof(double) * per_warp * warps;
+    size_t smem = sizeof(double) * per_warp * warps;
     int r;
     unsigned long long* next;
     if ((r = bufT(c, "dpnext", 1, &next))) return r;
     FSM_CUDA_TRY(cudaMemsetAsync(next, 0, sizeof(unsigned long long), c->stream));
     job.next = next;
     job.gwork = nullptr;
+    job.force_exact = c->dp_exact ? 1 : 0;
     const void* kf = job.q.metric == DTW ? (const void*)k_dp<DTW>
                    : job.q.metric == ERP ? (const void*)k_dp<ERP>
                    : job.q.metric == EDR ? (const void*)k_dp<EDR>
                    : job.q.metric == LCSS ? (const void*)k_dp<LCSS> : (const void*)k_dp<MSM>;
     unsigned grid;
     if (smem > (size_t)c->smem_optin - 4096) {
-        grid = (unsigned)c->sm_count * 2;
+        // band scratch in global memory (L2-resident per warp): 16 warps per SM
+        const long long want = (expected + warps * 32 - 1) / (warps * 32);
+        grid = (unsigned)std::max<long long>(1, std::min<long long>(want, (long long)c->sm_count * (16 / warps)));
         double* gw;
         if ((r = bufT(c, "dpwork", per_warp * warps * grid, &gw))) return r;
         job.gwork = gw;
-        smem = sizeof(double) * (((size_t)job.q.m + 1) & ~(size_t)1);
+        smem = 0;
     }
     switch (job.q.metric) {
         case DTW: if ((r = allow_smem(c, k_dp<DTW>, smem))) return r; break;
@@ -852,6 +858,7 @@ static int open_common(int device, fsmeld_ctx** out) {
     if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaGetDeviceProperties", __FILE__, __LINE__); }
     c->sm_count = prop.multiProcessorCount;
     c->smem_optin = (int)prop.sharedMemPerBlockOptin;
+    if (const char* ex = getenv("FSMELD_DP_EXACT")) c->dp_exact = ex[0] == '1';
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
         delete c;

@@ -1,15 +1,35 @@
 // Exact banded elastic distances (src/ElasticMeasures.cpp:24-198, dispatch
 // src/fsmeld.cpp:170-183) for candidate windows, one lane per candidate.
 //
-// Each lane keeps the previous and current band rows (offsets d = j - i + w,
-// 2w+1 cells) and a ring of its z-normalised candidate points in shared
-// memory laid out [slot][lane].  Every cell is computed from its three
-// neighbours with the reference's formula and operand order; out-of-band
-// neighbours read the reference's sentinels (1e18 for DTW/ERP/EDR/MSM, 0 for
-// LCSS) and the row-0 / column-0 boundary cells follow the reference's
-// initialisation loops.  A cell depends only on its neighbours, so the rows
-// give the reference's bits.  Candidate points are normalised once each, as
+// Each lane keeps one band row (offsets d = j - i + w, 2w+1 cells, updated in
+// place: cell d of the previous row is the diagonal neighbour of cell d and
+// the upper neighbour of cell d-1) and a power-of-two ring of its z-normalised
+// candidate points, both in shared memory laid out [slot][lane] so lanes never
+// share a bank word.  Candidate points are normalised once each, as
 // (t - mu) / sigma (src/fsmeld.cpp:823-826, 1202-1204).
+//
+// Every in-band cell is computed from its three neighbours with the
+// reference's formula and operand order.  The reference reads MAX_VAL = 1e18
+// (0 for LCSS) for neighbours outside the band; its column 0 of ERP/EDR/MSM
+// has its own formula.  Two modes reproduce that:
+//
+//  * fast mode (every lane, every row, one code path): the ring holds +-1e300
+//    for candidate columns outside the matrix, so cells outside the band come
+//    out >= 1e18 (0 for LCSS) without a per-cell test, and the column-0 cells
+//    reduce to the reference's column formula because their other two terms
+//    are >= 1e18.  This equals the reference bit for bit while every in-band
+//    value stays below 1e17, which holds when every cost term is below
+//    1e17 / (2m+2): guaranteed when |y| <= ylim for every candidate point,
+//    ylim = sqrt(1e17 / (2m+2)) - max|x| - |arg| - 2 (EDR/LCSS values are
+//    match counts, always in range).
+//  * exact mode (a candidate with a point beyond ylim, or a query whose
+//    ylim <= 0): the candidate restarts and every row clips the cells outside
+//    the band to the sentinel and evaluates column 0 with the reference's
+//    column formula, so sentinels are read exactly where the reference reads
+//    them whatever the magnitudes.
+//
+// DTW/LCSS start from a virtual cell (-1,-1) of value 0, which makes cell
+// (0,0) its own point distance (or match).
 //
 // Lanes are independent: each lane advances its own candidate one row per
 // step and, when its candidate finishes, takes the next one from a global
@@ -23,8 +43,9 @@
 // it has done.  A candidate whose bound already exceeds the cutoff (with a
 // 1e-9 relative slack for round-off) cannot be kept and stops.  For LCSS the
 // final match count is at most the row maximum plus the matches the
-// remaining rows can still reach.  Results are unchanged: only candidates
-// that would be discarded stop early.
+// remaining rows can still reach.  Out-of-band cells can only lower a row
+// minimum (raise an LCSS row maximum), which keeps the bound valid.  Results
+// are unchanged: only candidates that would be discarded stop early.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -32,7 +53,13 @@ namespace fsm {
 
 namespace {
 
+constexpr double kPad = 1e300;  // candidate points outside the matrix (fast mode)
+
 __device__ __forceinline__ double fmin3(double a, double b, double c) { return fmin(fmin(a, b), c); }
+
+// Cascading abandon margin: the bound and the DP carry independent round-off
+// (relative ~1e-13); a 1e-9 relative slack keeps the test conservative.
+__device__ __forceinline__ double slack(double cut) { return cut + 1e-9 * (1.0 + fabs(cut)); }
 
 // src/ElasticMeasures.cpp:173-176
 __device__ __forceinline__ double msm_c(double np, double x, double y, double c) {
@@ -41,99 +68,172 @@ __device__ __forceinline__ double msm_c(double np, double x, double y, double c)
     return dadd(c, (b < a) ? b : a);
 }
 
-// Cascading abandon margin: the bound and the DP carry independent round-off
-// (relative ~1e-13); a 1e-9 relative slack keeps the test conservative.
-__device__ __forceinline__ double slack(double cut) { return cut + 1e-9 * (1.0 + fabs(cut)); }
-
-struct Lane {
-    double* P;   // previous row [W2][32]
-    double* Cu;  // current row  [W2][32]
-    double* R;   // candidate ring [RING][32]
-    int lane;
-    __device__ double& p(int d) const { return P[d * 32 + lane]; }
-    __device__ double& cu(int d) const { return Cu[d * 32 + lane]; }
-    __device__ double& r(int s) const { return R[s * 32 + lane]; }
+// Per-row constants of the query point the row aligns.
+struct RowCtx {
+    double xi;   // query point of the row
+    double c0;   // ERP: dist(x, g); MSM: |x_i - x_{i-1}|
+    double xp;   // MSM: x_{i-1}
+    int i;       // row
 };
+
+// One band row in place.  A: band row [d * 32], A[W2 * 32] is a permanent
+// out-of-band cell; R: ring [slot * 32], RM = ring size - 1; s0: ring index
+// of the candidate column read by cell d = 0 (the column itself for
+// DTW/LCSS/MSM, column j-1 for ERP/EDR).  Returns the row minimum (maximum
+// for LCSS).  EXACT: clip cells outside [dlo, dhi] to the sentinel and use
+// the reference's column-0 formula (cell d0 = w - i).
+template <int METRIC, bool EXACT>
+__device__ __forceinline__ double dp_row(double* __restrict__ A, const double* __restrict__ R, int RM, int W2,
+                                         int s0, const RowCtx& rc, double arg, int dlo, int dhi, int d0) {
+    constexpr double SENT = (METRIC == LCSS) ? 0.0 : kDpMax;
+    const double xi = rc.xi;
+    double left = SENT, ext = SENT;
+    double pd = A[0];
+    double yprev = (METRIC == MSM) ? R[((s0 - 1) & RM) * 32] : 0.0;  // y_{j-1} for MSM
+    const bool ge = rc.xp <= xi, le = xi <= rc.xp;
+#pragma unroll 3
+    for (int d = 0; d < W2; ++d) {
+        const double pn = A[(d + 1) * 32];
+        const double y = R[((s0 + d) & RM) * 32];
+        double v;
+        if (METRIC == DTW) {
+            v = dadd(fmin3(pn, left, pd), dsq(xi, y));
+        } else if (METRIC == ERP) {  // y = y[j-1]
+            const double match = dadd(pd, dsq(xi, y));
+            const double ins = dadd(left, dsq(y, arg));
+            const double del = dadd(pn, rc.c0);
+            v = fmin3(match, ins, del);
+            if (EXACT && d == d0) v = del;                       // cur[0] = prev[0] + dist(x, g)
+        } else if (METRIC == EDR) {  // y = y[j-1]
+            const double sub = (fabs(dsub(xi, y)) <= arg) ? 0.0 : 1.0;
+            v = fmin3(dadd(pn, 1.0), dadd(left, 1.0), dadd(pd, sub));
+            if (EXACT && d == d0) v = (double)rc.i;              // cur[0] = i
+        } else if (METRIC == LCSS) {
+            double best = (fabs(dsub(xi, y)) <= arg) ? dadd(pd, 1.0) : pd;
+            if (best < pn) best = pn;
+            if (best < left) best = left;
+            v = best;
+        } else {  // MSM, y = y_j, yprev = y_{j-1}
+            const double axy = fabs(dsub(xi, y));
+            const double c1 = dadd(pd, axy);
+            // C(x_i, x_{i-1}, y_j): x_i lies between x_{i-1} and y_j
+            const bool b2 = (ge && xi <= y) || (y <= xi && le);
+            const double c2 = dadd(pn, b2 ? arg : dadd(arg, fmin(rc.c0, axy)));
+            // C(y_j, x_i, y_{j-1}): y_j lies between x_i and y_{j-1}
+            const bool b3 = (xi <= y && y <= yprev) || (yprev <= y && y <= xi);
+            const double c3 = dadd(left, b3 ? arg : dadd(arg, fmin(axy, fabs(dsub(y, yprev)))));
+            v = fmin3(c1, c2, c3);
+            if (EXACT && d == d0) v = dadd(pn, msm_c(xi, rc.xp, y, arg));  // column 0
+            yprev = y;
+        }
+        if (EXACT && (d < dlo || d > dhi)) v = SENT;
+        A[d * 32] = v;
+        left = v;
+        pd = pn;
+        ext = (METRIC == LCSS) ? fmax(ext, v) : fmin(ext, v);
+    }
+    return ext;
+}
 
 }  // namespace
 
 template <int METRIC>
-__global__ void __launch_bounds__(128) k_dp(Geom g, DpJob job) {
+__global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
     extern __shared__ __align__(16) double dp_smem[];
     const QueryDev& q = job.q;
     const int m = q.m, w = q.w;
-    const int W2 = 2 * w + 1, RING = 2 * w + 2;
+    const int W2 = 2 * w + 1;
+    const int RING = dp_ring(w), RM = RING - 1;
     const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double* X = dp_smem;
-    for (int i = threadIdx.x; i < m; i += blockDim.x) X[i] = q.qn[i];
-    const size_t per_warp = (size_t)(2 * W2 + RING) * 32;
+    const double* __restrict__ X = q.qn;
+    const size_t per_warp = dp_warp_doubles(w);
     double* wbase = job.gwork ? job.gwork + ((size_t)blockIdx.x * warps + warp) * per_warp
-                              : dp_smem + ((m + 1) & ~1) + warp * per_warp;
-    __syncthreads();
-    Lane B{wbase, wbase + (size_t)W2 * 32, wbase + (size_t)2 * W2 * 32, lane};
+                              : dp_smem + warp * per_warp;
+    double* const A = wbase + lane;                            // band row, A[d * 32], d in [0, W2]
+    double* const R = wbase + (size_t)(W2 + 1) * 32 + lane;    // ring, R[slot * 32]
     const unsigned long long n_all = job.list ? *job.n_list : (unsigned long long)job.n_windows;
     const unsigned long long n =
         (job.list && n_all > (unsigned long long)job.list_cap) ? job.list_cap : n_all;
     const double cut = job.cutoff;
     const double arg = q.arg;
+    constexpr bool ONE_BASED = (METRIC == ERP || METRIC == EDR);  // rows 1..m, columns 0..m
+    constexpr double SENT = (METRIC == LCSS) ? 0.0 : kDpMax;
+    const int last = ONE_BASED ? m : m - 1;  // last row and last column
+
+    // fast-mode limit on candidate points (see the header)
+    double ylim;
+    if (METRIC == EDR) {
+        ylim = INFINITY;
+    } else if (METRIC == LCSS) {
+        ylim = (fabs(arg) < 1e299) ? INFINITY : -1.0;  // padding must never match
+    } else {
+        double xm = 0.0;
+        for (int k = lane; k < m; k += 32) xm = fmax(xm, fabs(X[k]));
+        for (int o = 16; o; o >>= 1) xm = fmax(xm, __shfl_xor_sync(0xffffffffu, xm, o));
+        ylim = sqrt(1e17 / (2.0 * m + 2.0)) - xm - fabs(arg) - 2.0;
+    }
+    const bool query_exact = job.force_exact || !(ylim > 0.0);
 
     // per-lane candidate state
     bool active = false;
+    bool exact = query_exact;  // exact mode for the lane's candidate
+    bool over = false;         // a candidate point exceeded ylim (fast mode)
     long long gi = 0;
     const double* tp = job.target;
     const double* lr = job.lraw;
     const double* ur = job.uraw;
     double mu = 0.0, sg = 1.0;
     int row = 0, ny = 0;
-    double col = 0.0;  // ERP/EDR: previous row's column 0; MSM: running column 0
     double Ssum = 0.0, Pre = 0.0;  // GLB Q->T sum of the candidate, and its prefix over rows done
-    bool has_s = false;            // the candidate came with a GLB Q->T sum
+    bool has_s = false;
 
-    auto y_at = [&](int j) { return ddiv(dsub(tp[j], mu), sg); };
-    auto ring_slot = [&](int j) { int s = j % RING; return s < 0 ? s + RING : s; };
-    auto fill_ring = [&](int upto) {  // candidate points 0..upto into the ring
-        for (; ny <= upto; ++ny) B.r(ring_slot(ny)) = y_at(ny);
+    // candidate points ny..upto into the ring; columns past the window are padding
+    auto fill_ring = [&](int upto) {
+        for (; ny <= upto; ++ny) {
+            double y = kPad;
+            if (ny < m) {
+                y = ddiv(dsub(tp[ny], mu), sg);
+                over = over || !(fabs(y) <= ylim);
+            }
+            R[(ny & RM) * 32] = y;
+        }
     };
 
-    // row-0 set-up per metric (the reference's initialisation loops)
+    // band before the first general row (the reference's initialisation loops)
     auto start = [&]() {
         ny = 0;
+        over = false;
+        Pre = 0.0;
+        for (int d = 0; d <= W2; ++d) A[d * 32] = SENT;
+        for (int c = -w - 1; c < 0; ++c) R[(c & RM) * 32] = -kPad;  // columns left of the matrix
         switch (METRIC) {
-            case DTW:
-                for (int d = 0; d < W2; ++d) B.p(d) = kDpMax;
+            case DTW:  // virtual (-1,-1) = 0 feeds cell (0,0)
+            case LCSS:
+                A[w * 32] = 0.0;
                 row = 0;
                 break;
             case ERP: {  // prev[0] = 0, prev[j] = prev[j-1] + dist(y[j-1], g), j <= min(m, w)
-                for (int d = 0; d < W2; ++d) B.p(d) = kDpMax;
+                A[w * 32] = 0.0;
                 double acc = 0.0;
                 for (int j = 1; j <= min(m, w); ++j) {
                     fill_ring(j - 1);
-                    acc = dadd(acc, dsq(B.r(ring_slot(j - 1)), arg));
-                    B.p(j + w) = acc;
+                    acc = dadd(acc, dsq(R[((j - 1) & RM) * 32], arg));
+                    A[(j + w) * 32] = acc;
                 }
-                col = 0.0;
                 row = 1;
                 break;
             }
-            case EDR:
-                for (int d = 0; d < W2; ++d) B.p(d) = kDpMax;
-                for (int j = 1; j <= min(m, w); ++j) B.p(j + w) = (double)j;
-                col = 0.0;
+            case EDR:  // prev[j] = j, j <= min(m, w)
+                for (int j = 0; j <= min(m, w); ++j) A[(j + w) * 32] = (double)j;
                 row = 1;
                 break;
-            case LCSS:
-                for (int d = 0; d < W2; ++d) B.p(d) = 0.0;
-                row = 0;
-                break;
             default: {  // MSM row 0: cost[0] = |x0-y0|, cost[j] = cost[j-1] + C(y_j, x_0, y_{j-1})
-                for (int d = 0; d < W2; ++d) B.p(d) = kDpMax;
                 fill_ring(min(m - 1, w));
-                double acc = fabs(dsub(X[0], B.r(0)));
-                col = acc;
-                B.p(w) = acc;
+                double acc = fabs(dsub(X[0], R[0]));
+                A[w * 32] = acc;
                 for (int j = 1; j < m && j <= w; ++j) {
-                    acc = dadd(acc, msm_c(B.r(ring_slot(j)), X[0], B.r(ring_slot(j - 1)), arg));
-                    B.p(j + w) = acc;
+                    acc = dadd(acc, msm_c(R[(j & RM) * 32], X[0], R[((j - 1) & RM) * 32], arg));
+                    A[(j + w) * 32] = acc;
                 }
                 row = 1;
                 break;
@@ -169,7 +269,7 @@ __global__ void __launch_bounds__(128) k_dp(Geom g, DpJob job) {
                         ++valid_count;
                         has_s = job.list_s && job.lraw && job.list_s[c] >= 0.0;
                         Ssum = has_s ? job.list_s[c] : 0.0;
-                        Pre = 0.0;
+                        exact = query_exact;
                         start();
                         active = true;
                     }
@@ -180,192 +280,70 @@ __global__ void __launch_bounds__(128) k_dp(Geom g, DpJob job) {
             if (drained) break;
             continue;
         }
-        if (active) {
-            bool done = false, keep = false;
-            double dist = 0.0;
-            const int i = row;
-            switch (METRIC) {
-                case DTW: {
-                    fill_ring(min(m - 1, i + w));
-                    const double xi = X[i];
-                    double left = kDpMax, rmin = kDpMax;
-                    int sl = ring_slot(i - w);
-                    for (int d = 0; d < W2; ++d, sl = (sl + 1 == RING) ? 0 : sl + 1) {
-                        const int j = i - w + d;
-                        double v = kDpMax;
-                        if (j >= 0 && j < m) {
-                            const double yv0 = B.r(sl);
-                            const double dd = dsq(xi, yv0);
-                            if (i == 0 && j == 0) {
-                                v = dd;
-                            } else {
-                                const double yv = (j == 0 || d == 0) ? kDpMax : left;
-                                const double xv = (i == 0 || d + 1 > 2 * w) ? kDpMax : B.p(d + 1);
-                                const double zv = (i == 0 || j == 0) ? kDpMax : B.p(d);
-                                v = dadd(fmin3(xv, yv, zv), dd);
-                            }
-                            rmin = fmin(rmin, v);
-                        }
-                        B.cu(d) = v;
-                        left = v;
-                    }
-                    if (has_s && i >= 1 && i <= m - 2) Pre = dadd(Pre, qt_term(DTW, xi, i, m, w, tp, lr, ur, mu, sg, arg));
-                    if (i == m - 1) {
-                        const double fin = B.cu(w);
-                        dist = isfinite(fin) ? dsqrt(dmax0(fin)) : kDpMax;
-                        done = true;
-                        keep = dist <= cut;
-                    } else if (dsqrt(dmax0(dadd(rmin, fmax(0.0, dsub(Ssum, Pre))))) > slack(cut)) {
-                        done = true;
-                    }
-                    break;
-                }
-                case ERP:
-                case EDR: {
-                    fill_ring(min(m, i + w) - 1);
-                    const double xi = X[i - 1];
-                    const double dxg = (METRIC == ERP) ? dsq(xi, arg) : 1.0;
-                    const double cur_col0 = (i <= w) ? ((METRIC == ERP) ? dadd(col, dxg) : (double)i) : kDpMax;
-                    double rmin = cur_col0;
-                    const int lo = max(1, i - w);
-                    double left = kDpMax;
-                    int sl = ring_slot(i - w - 1);
-                    for (int d = 0; d < W2; ++d, sl = (sl + 1 == RING) ? 0 : sl + 1) {
-                        const int j = i - w + d;
-                        double v = kDpMax;
-                        if (j >= lo && j <= m) {
-                            if (j == lo) left = (j - 1 == 0) ? cur_col0 : kDpMax;
-                            const double yj1 = B.r(sl);
-                            const double up = (d + 1 <= 2 * w) ? B.p(d + 1) : kDpMax;
-                            const double dg = (j - 1 == 0) ? col : B.p(d);
-                            if (METRIC == ERP) {
-                                const double match = dadd(dg, dsq(xi, yj1));
-                                const double ins = dadd(left, dsq(yj1, arg));
-                                const double del = dadd(up, dxg);
-                                v = fmin3(match, ins, del);
-                            } else {
-                                const double sub = (fabs(dsub(xi, yj1)) <= arg) ? 0.0 : 1.0;
-                                v = fmin3(dadd(up, 1.0), dadd(left, 1.0), dadd(dg, sub));
-                            }
-                            rmin = fmin(rmin, v);
-                        }
-                        B.cu(d) = v;
-                        left = v;
-                    }
-                    col = cur_col0;
-                    if (has_s && i - 1 >= 1 && i - 1 <= m - 2) Pre = dadd(Pre, qt_term(METRIC, xi, i - 1, m, w, tp, lr, ur, mu, sg, arg));
-                    if (i == m) {
-                        const double res = B.cu(w);
-                        if (METRIC == ERP) dist = isfinite(res) ? dsqrt(dmax0(res)) : kDpMax;
-                        else dist = res;
-                        done = true;
-                        keep = dist <= cut;
-                    } else {
-                        const double bnd = dadd(rmin, fmax(0.0, dsub(Ssum, Pre)));
-                        if ((METRIC == ERP ? dsqrt(dmax0(bnd)) : bnd) > slack(cut)) done = true;
-                    }
-                    break;
-                }
-                case LCSS: {
-                    fill_ring(min(m - 1, i + w));
-                    const double xi = X[i];
-                    const int wmin = max(0, i - w), wmax = min(m - 1, i + w);
-                    double left = 0.0, rmax = 0.0;
-                    int sl = ring_slot(i - w);
-                    for (int d = 0; d < W2; ++d, sl = (sl + 1 == RING) ? 0 : sl + 1) {
-                        const int j = i - w + d;
-                        double v = 0.0;
-                        if (j >= wmin && j <= wmax) {
-                            const double yv0 = B.r(sl);
-                            const bool hit = fabs(dsub(xi, yv0)) <= arg;
-                            if (i + j == 0) {
-                                v = hit ? 1.0 : 0.0;
-                            } else if (i == 0) {
-                                v = hit ? 1.0 : ((j > wmin) ? left : 0.0);
-                            } else if (j == 0) {
-                                v = hit ? 1.0 : B.p(d + 1);
-                            } else {
-                                const double v1 = B.p(d);
-                                const double v2 = (d + 1 <= 2 * w) ? B.p(d + 1) : 0.0;
-                                const double v3 = (j > wmin) ? left : 0.0;
-                                double best = hit ? dadd(v1, 1.0) : v1;
-                                if (best < v2) best = v2;
-                                if (best < v3) best = v3;
-                                v = best;
-                            }
-                            rmax = fmax(rmax, v);
-                        }
-                        B.cu(d) = v;
-                        left = v;
-                    }
-                    if (has_s) Pre = dadd(Pre, qt_term(LCSS, xi, i, m, w, tp, lr, ur, mu, sg, arg));
-                    if (i == m - 1) {
-                        dist = dsub(1.0, ddiv(B.cu(w), (double)m));
-                        done = true;
-                        keep = dist <= cut;
-                    } else {
-                        // remaining rows can add at most one match each, and only where the
-                        // query point meets the candidate envelope
-                        double rest = (double)(m - 1 - i);
-                        if (has_s) rest = fmin(rest, fmax(0.0, dsub(Ssum, Pre)));
-                        if (dsub(1.0, ddiv(dadd(rmax, rest), (double)m)) > slack(cut)) done = true;
-                    }
-                    break;
-                }
-                default: {  // MSM
-                    fill_ring(min(m - 1, i + w));
-                    const double xi = X[i], xi1 = X[i - 1];
-                    double colv = kDpMax;
-                    if (i <= w) {
-                        col = dadd(col, msm_c(xi, xi1, B.r(0), arg));
-                        colv = col;
-                    }
-                    const int js = max(1, i - w), je = min(m - 1, i + w);
-                    double left = kDpMax, rmin = colv;
-                    int sl = ring_slot(i - w);
-                    for (int d = 0; d < W2; ++d, sl = (sl + 1 == RING) ? 0 : sl + 1) {
-                        const int j = i - w + d;
-                        double v = kDpMax;
-                        if (j == 0) {
-                            v = colv;  // column 0 (in band only while i <= w)
-                        } else if (j >= js && j <= je) {
-                            if (j == js) left = (j - 1 == 0) ? colv : kDpMax;
-                            const double yj = B.r(sl);
-                            const double yj1 = B.r(sl == 0 ? RING - 1 : sl - 1);
-                            const double c1 = dadd(B.p(d), fabs(dsub(xi, yj)));
-                            const double c2 = dadd((d + 1 <= 2 * w) ? B.p(d + 1) : kDpMax, msm_c(xi, xi1, yj, arg));
-                            const double c3 = dadd(left, msm_c(yj, xi, yj1, arg));
-                            v = fmin3(c1, c2, c3);
-                            rmin = fmin(rmin, v);
-                        }
-                        B.cu(d) = v;
-                        left = v;
-                    }
-                    if (has_s && i >= 1 && i <= m - 2) Pre = dadd(Pre, qt_term(MSM, xi, i, m, w, tp, lr, ur, mu, sg, arg));
-                    if (i == m - 1) {
-                        dist = B.cu(w);
-                        done = true;
-                        keep = dist <= cut;
-                    } else if (dadd(rmin, fmax(0.0, dsub(Ssum, Pre))) > slack(cut)) {
-                        done = true;
-                    }
-                    break;
+        if (!active) continue;
+
+        const int i = row;
+        const int s0 = ONE_BASED ? i - w - 1 : i - w;  // ring index read by cell d = 0
+        fill_ring(s0 + 2 * w);                          // one new point per row in steady state
+        if (over && !exact) {                           // out of the fast-mode range: restart exact
+            exact = true;
+            start();
+            continue;
+        }
+        const int k = ONE_BASED ? i - 1 : i;  // query index aligned by this row
+        RowCtx rc;
+        rc.xi = X[k];
+        rc.c0 = 0.0;
+        rc.xp = rc.xi;
+        rc.i = i;
+        if (METRIC == ERP) rc.c0 = dsq(rc.xi, arg);
+        if (METRIC == MSM) {
+            rc.xp = X[i - 1];
+            rc.c0 = fabs(dsub(rc.xi, rc.xp));
+        }
+        // cascading-bound term of this row's query point
+        const bool use_term = has_s && (METRIC == LCSS || (k >= 1 && k <= m - 2));
+        const double term = use_term ? qt_term(METRIC, rc.xi, k, m, w, tp, lr, ur, mu, sg, arg) : 0.0;
+        double ext;
+        if (!exact) {
+            ext = dp_row<METRIC, false>(A, R, RM, W2, s0, rc, arg, 0, 0, -1);
+        } else {
+            const int dlo = max(0, w - i), dhi = min(2 * w, last - i + w);
+            const int d0 = (METRIC == ERP || METRIC == EDR || METRIC == MSM) ? w - i : -1;
+            ext = dp_row<METRIC, true>(A, R, RM, W2, s0, rc, arg, dlo, dhi, d0);
+        }
+        if (use_term) Pre = dadd(Pre, term);
+
+        bool done = false, keep = false;
+        double dist = 0.0;
+        if (i == last) {
+            const double fin = A[w * 32];
+            if (METRIC == DTW || METRIC == ERP) dist = isfinite(fin) ? dsqrt(dmax0(fin)) : kDpMax;
+            else if (METRIC == LCSS) dist = dsub(1.0, ddiv(fin, (double)m));
+            else dist = fin;
+            done = true;
+            keep = dist <= cut && isfinite(dist);
+        } else if (METRIC == LCSS) {
+            // remaining rows can add at most one match each, and only where the
+            // query point meets the candidate envelope
+            double rest = (double)(m - 1 - i);
+            if (has_s) rest = fmin(rest, fmax(0.0, dsub(Ssum, Pre)));
+            if (dsub(1.0, ddiv(dadd(ext, rest), (double)m)) > slack(cut)) done = true;
+        } else {
+            const double bnd = dadd(ext, fmax(0.0, dsub(Ssum, Pre)));
+            if ((METRIC == DTW || METRIC == ERP ? dsqrt(dmax0(bnd)) : bnd) > slack(cut)) done = true;
+        }
+        if (done) {
+            active = false;
+            if (keep) {
+                const unsigned long long o = atomicAdd(job.n_out, 1ull);
+                if (o < (unsigned long long)job.out_cap) {
+                    job.out_idx[o] = gi;
+                    job.out_dist[o] = dist;
                 }
             }
-            if (done) {
-                active = false;
-                keep = keep && isfinite(dist);
-                if (keep) {
-                    const unsigned long long o = atomicAdd(job.n_out, 1ull);
-                    if (o < (unsigned long long)job.out_cap) {
-                        job.out_idx[o] = gi;
-                        job.out_dist[o] = dist;
-                    }
-                }
-            } else {
-                double* t = B.P; B.P = B.Cu; B.Cu = t;
-                ++row;
-            }
+        } else {
+            ++row;
         }
     }
     if (job.n_valid) {
@@ -374,7 +352,13 @@ __global__ void __launch_bounds__(128) k_dp(Geom g, DpJob job) {
     }
 }
 
-size_t dp_warp_doubles(int w) { return (size_t)(2 * (2 * w + 1) + (2 * w + 2)) * 32; }
+__host__ __device__ int dp_ring(int w) {
+    int r = 1;
+    while (r < 2 * w + 2) r <<= 1;
+    return r;
+}
+
+__host__ __device__ size_t dp_warp_doubles(int w) { return (size_t)((2 * w + 2) + dp_ring(w)) * 32; }
 
 template __global__ void k_dp<DTW>(Geom, DpJob);
 template __global__ void k_dp<ERP>(Geom, DpJob);

@@ -69,6 +69,7 @@ struct DpJob {
     unsigned long long* n_valid;
     unsigned long long* next;   // work counter (zeroed before the launch)
     double* gwork;              // global band scratch when shared memory is too small
+    int force_exact;            // every candidate in the DP's exact boundary mode
 };
 
 __global__ void k_mvmean(const double* __restrict__ target, Geom g, double* __restrict__ mu,
@@ -101,6 +102,11 @@ template <int T, int IPT>
 size_t threshold_sort_tmp_bytes();
 size_t lbip_smem_bytes(int P, int m_k, int m, int metric);
 int lbip_set_w16();
-size_t dp_warp_doubles(int w);
+// DP block size (2 warps: the per-warp band scratch sets the occupancy)
+constexpr int kDpThreads = 64;
+// DP per-warp scratch: band row (2w+1 cells + one out-of-band cell) and the
+// candidate ring (power of two >= 2w+2 points), 32 lanes each
+__host__ __device__ int dp_ring(int w);
+__host__ __device__ size_t dp_warp_doubles(int w);
 
 }  // namespace fsm

@@ -176,8 +176,8 @@ extern "C" int fsmeld_exact_noalloc(int device, const double* device_target, int
     double* win = (double*)(base + kOffWin);
 
     // band rows in shared memory only (no global spill buffer on this path)
-    const int warps = 4;
-    const size_t smem = sizeof(double) * ((((size_t)m + 1) & ~(size_t)1) + dp_warp_doubles(w) * warps);
+    const int warps = kDpThreads / 32;
+    const size_t smem = sizeof(double) * dp_warp_doubles(w) * warps;
     int dev_optin = 0;
     if ((e = cudaDeviceGetAttribute(&dev_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device)) != cudaSuccess)
         return cuda_fail(e, "cudaDeviceGetAttribute", __FILE__, __LINE__);

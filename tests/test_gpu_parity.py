@@ -244,3 +244,52 @@ def test_errors(api):
         with pytest.raises(api.FsmeldError) as ei:
             e.cutoff(q, 32, 5, "dtw", 3, 0.0, exclude=(0, 2000))
         assert ei.value.status == api.E_FEWER_K
+
+
+def _znorm_max(q):
+    q = np.asarray(q, dtype=np.float64)
+    return float(np.max(np.abs((q - q.mean()) / q.std())))
+
+
+def _all_distances(api, oracle, t, q, m, w, metric, arg):
+    with api.Engine(t) as e:
+        gidx, gdist, gc = e.exact(q, m, 1e300, metric, w, arg)
+    oidx, odist, oc = oracle.exact(t, q, m, 1e300, metric, w, arg)
+    assert len(oidx) == oc["valid"]  # every valid window is reported
+    assert list(gidx) == list(oidx), metric
+    assert bits_equal(gdist, odist), metric
+    assert gc["valid"] == oc["valid"]
+
+
+@pytest.mark.parametrize("metric,arg", METRIC_ARGS)
+def test_all_window_distances_bits(api, oracle, structured, metric, arg):
+    # the full distance profile (every valid window), through the DP's fast mode
+    t, q, m, w = structured
+    _all_distances(api, oracle, t, q, m, w, metric, arg)
+
+
+@pytest.mark.parametrize("metric", ["erp", "msm"])
+@pytest.mark.parametrize("margin", [1.5, -1e9])
+def test_dp_exact_boundary_mode(api, oracle, structured, metric, margin):
+    # An ERP gap value g or MSM cost c near sqrt(1e17 / (2m+2)) makes the DP's
+    # fast-mode limit on candidate points small (margin 1.5: lanes whose
+    # candidate has a point above ~1.5 restart in the exact mode while the
+    # others stay fast) or negative (the whole query runs in the exact mode).
+    # Cell values reach ~1e16 and column 0 of ERP/MSM takes the reference's
+    # column formula; every distance must still equal the oracle's bits.
+    t, q, m, w = structured
+    big = np.sqrt(1e17 / (2.0 * m + 2.0)) - _znorm_max(q[:m]) - 2.0 - margin
+    _all_distances(api, oracle, t, q, m, w, metric, float(big))
+
+
+def test_dp_forced_exact_mode(api, oracle, structured, monkeypatch):
+    # FSMELD_DP_EXACT=1 runs every candidate in the exact boundary mode; the
+    # results are the same as the fast mode's
+    t, q, m, w = structured
+    monkeypatch.setenv("FSMELD_DP_EXACT", "1")
+    for metric, arg in METRIC_ARGS:
+        _all_distances(api, oracle, t, q, m, w, metric, arg)
+        with api.Engine(t) as e:
+            gidx, gdist, _ = e.cutoff(q, m, 9, metric, w, arg)
+        oidx, odist, _ = oracle.cutoff(t, q, m, 9, metric, w, arg)
+        assert list(gidx) == list(oidx) and bits_equal(gdist, odist), metric
