@@ -9,8 +9,9 @@
 // and a penalty sum C, and scores LB[i] = h(t_i) * g_i; the argmax gives t.
 //
 // Here one CTA handles one (segment, side):
-//  1. dedup with a block scan, sort runs with a block merge sort (total
-//     order: value, NaN last, ties by position);
+//  1. dedup with a block scan, sort runs with a block radix sort on an
+//     order-preserving 64-bit key (total order: value, NaN last, ties by
+//     position through the sort's stability);
 //  2. every pointer move of the sweep becomes an op with the sweep step at
 //     which it fires (a binary search over the sorted values); ops are
 //     ordered by (step, stream, rank) -- the order the reference's loops
@@ -24,7 +25,7 @@
 // to its heap layout; here equal keys pop by query index.  The threshold is
 // the same unless two candidates' scores tie to the last bit.
 #include <climits>
-#include <cub/block/block_merge_sort.cuh>
+#include <cub/block/block_radix_sort.cuh>
 #include <cub/block/block_reduce.cuh>
 #include <cub/block/block_scan.cuh>
 
@@ -37,29 +38,15 @@ namespace {
 
 constexpr int kNever = INT_MAX;
 
-struct RunKey {
-    double v;
-    int pos;
-    int cnt;
-};
-
-struct RunLess {
-    int desc;
-    __device__ bool operator()(const RunKey& a, const RunKey& b) const {
-        const bool na = isnan(a.v), nb = isnan(b.v);
-        if (na != nb) return nb;
-        if (!na) {
-            if (desc) {
-                if (a.v > b.v) return true;
-                if (a.v < b.v) return false;
-            } else {
-                if (a.v < b.v) return true;
-                if (a.v > b.v) return false;
-            }
-        }
-        return a.pos < b.pos;
-    }
-};
+// Order-preserving key of a double: ascending values map to ascending keys,
+// -0 and +0 to one key (they compare equal), NaN to the largest key (sorted
+// last); desc reverses the order of the non-NaN values.
+__device__ __forceinline__ unsigned long long order_key(double x, int desc) {
+    if (isnan(x)) return ~0ull;
+    const unsigned long long u = (unsigned long long)__double_as_longlong(x == 0.0 ? 0.0 : x);
+    const unsigned long long k = (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+    return desc ? ~k : k;
+}
 
 struct ArgMax {
     double v;
@@ -97,16 +84,6 @@ __device__ __forceinline__ int first_step(const double* tv, int n, Cmp c, double
     return lo < n ? lo : kNever;
 }
 
-__device__ __forceinline__ int lower_count(const double* a, int n, double x) {  // #(a < x), a ascending
-    int lo = 0, hi = n;
-    while (lo < hi) { const int mid = (lo + hi) >> 1; if (a[mid] < x) lo = mid + 1; else hi = mid; }
-    return lo;
-}
-__device__ __forceinline__ int upper_count(const double* a, int n, double x) {  // #(a <= x)
-    int lo = 0, hi = n;
-    while (lo < hi) { const int mid = (lo + hi) >> 1; if (a[mid] <= x) lo = mid + 1; else hi = mid; }
-    return lo;
-}
 // prefix length of an index-ordered table whose keys satisfy pred (monotone)
 template <typename F>
 __device__ __forceinline__ int prefix_count(int n, F pred) {
@@ -136,7 +113,7 @@ struct Plan {
 template <int T, int IPT>
 __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restrict__ jobs,
                                                  unsigned char* gwork, long long slot_stride) {
-    using Sort = cub::BlockMergeSort<RunKey, T, IPT>;
+    using Sort = cub::BlockRadixSort<unsigned long long, T, IPT, int>;
     using IScan = cub::BlockScan<int, T>;
     using AReduce = cub::BlockReduce<ArgMax, T>;
     constexpr int CAP = T * IPT;
@@ -145,8 +122,8 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
     __shared__ typename IScan::TempStorage iscan_tmp;
     __shared__ typename AReduce::TempStorage red_tmp;
     __shared__ int s_nr, s_nfin, s_best, s_nops;
-    __shared__ Plan s_plan;
-    __shared__ double s_t0;
+    __shared__ int s_cnt[2];
+    __shared__ double s_init[4];
 
     const ThrJob& job = jobs[blockIdx.y];
     const QueryDev& q = job.q;
@@ -156,16 +133,17 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
 
     unsigned char* base = gwork ? gwork + (long long)(blockIdx.y * gridDim.x + blockIdx.x) * slot_stride
                                 : thr_smem;
-    // region X: runs (phase 1) / sort temp (phase 2) / sorted values + g (phase 3)
-    const size_t xbytes = ((sizeof(typename Sort::TempStorage) > (size_t)CAP * 16 + 16
+    // runs (phases 1-3), then region X: sort temp (phase 2) / sorted values + g (phase 3)
+    double* rval = (double*)base;                                          // [CAP]
+    int* rstart = (int*)(base + (size_t)CAP * 8);                          // [CAP + 1]
+    unsigned char* xb = base + (((size_t)CAP * 12 + 4 + 15) & ~size_t(15));
+    const size_t xbytes = ((sizeof(typename Sort::TempStorage) > (size_t)CAP * 12 + 16
                                 ? sizeof(typename Sort::TempStorage)
-                                : (size_t)CAP * 16 + 16) + 15) & ~size_t(15);
-    double* rval = (double*)base;                       // [CAP]
-    int* rstart = (int*)(base + (size_t)CAP * 8);       // [CAP + 1]
-    typename Sort::TempStorage& sort_tmp = *reinterpret_cast<typename Sort::TempStorage*>(base);
-    double* tv = (double*)base;                         // [CAP] sorted values
-    int* gp = (int*)(base + (size_t)CAP * 8);           // [CAP] inclusive count sums
-    unsigned char* zb = base + xbytes;
+                                : (size_t)CAP * 12 + 16) + 15) & ~size_t(15);
+    typename Sort::TempStorage& sort_tmp = *reinterpret_cast<typename Sort::TempStorage*>(xb);
+    double* tv = (double*)xb;                           // [CAP] sorted values
+    int* gp = (int*)(xb + (size_t)CAP * 8);             // [CAP] inclusive count sums
+    unsigned char* zb = xb + xbytes;
     int* sA = (int*)zb;                                 // [m]
     int* sB = sA + m;                                   // [m]
     int* opdesc = sB + m;                               // [2m]
@@ -214,23 +192,33 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
         __syncthreads();
 
         // ---- 2. sort runs (src/find_t_lp.cpp:68-81)
-        RunKey keys[IPT];
+        unsigned long long keys[IPT];
+        int rid[IPT];
 #pragma unroll
         for (int k = 0; k < IPT; ++k) {
             const int r = t * IPT + k;
-            if (r < nr) keys[k] = RunKey{rval[r], r, rstart[r + 1] - rstart[r]};
-            else keys[k] = RunKey{dnan(), INT_MAX, 0};
+            keys[k] = (r < nr) ? order_key(rval[r], upper ? 0 : 1) : ~0ull;  // padding after every run
+            rid[k] = r;
         }
-        __syncthreads();
-        Sort(sort_tmp).Sort(keys, RunLess{upper ? 0 : 1}, nr, RunKey{dnan(), INT_MAX, 0});
+        Sort(sort_tmp).Sort(keys, rid);
         __syncthreads();
 
         // ---- 3. sorted values, cumulative counts g_i, finite prefix length
         int csum = 0, nf = 0;
+        double sv_[IPT];
+        int sc_[IPT];
 #pragma unroll
         for (int k = 0; k < IPT; ++k) {
             const int i = t * IPT + k;
-            if (i < nr) { csum += keys[k].cnt; nf += isnan(keys[k].v) ? 0 : 1; }
+            sv_[k] = 0.0;
+            sc_[k] = 0;
+            if (i < nr) {
+                const int r = rid[k];
+                sv_[k] = rval[r];
+                sc_[k] = rstart[r + 1] - rstart[r];
+                csum += sc_[k];
+                nf += isnan(sv_[k]) ? 0 : 1;
+            }
         }
         int cbase;
         IScan(iscan_tmp).ExclusiveSum(csum, cbase);
@@ -241,12 +229,12 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
         for (int k = 0; k < IPT; ++k) {
             const int i = t * IPT + k;
             if (i < nr) {
-                tv[i] = keys[k].v;
-                cbase += keys[k].cnt;
+                tv[i] = sv_[k];
+                cbase += sc_[k];
                 gp[i] = cbase;
             }
         }
-        if (t == 0) s_nfin = nfin_total;
+        if (t == 0) { s_nfin = nfin_total; s_cnt[0] = 0; s_cnt[1] = 0; }
         __syncthreads();
         const int nfin = s_nfin;
         double* out = job.thr + s * 2 + upper;
@@ -256,49 +244,59 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
             continue;
         }
 
-        // ---- 4. stream plan (one thread), src/find_t_lp.cpp init loops
-        if (t == 0) {
-            const double t0 = tv[0];
-            Plan pl;
-            pl.kind = kind; pl.upper = upper; pl.p = p;
-            pl.idx1 = pl.idx2 = pl.kA0 = pl.kB0 = 0;
-            pl.nA = pl.nB = 0;
+        // ---- 4. stream plan, src/find_t_lp.cpp init loops: the pointer
+        // scans stop at the partition point of a monotone table (sorted
+        // query, t_l/t_u of the sorted query, the ERP pop orders), found here
+        // as a block-wide count
+        const double t0 = tv[0];
+        {
+            int c0 = 0, c1 = 0;
+            for (int j = t; j < m; j += T) {
+                if (kind == 0) {
+                    c0 += upper ? (q.qs[j] <= t0) : (q.qs[j] < t0);
+                } else if (kind == 1) {
+                    if (!upper) { c0 += q.qs[j] < t0; c1 += q.tlq[j] < t0; }
+                    else { c0 += q.qs[j] <= t0; c1 += q.tuq[j] <= t0; }
+                } else {
+                    if (!upper) { c0 += q.otl[q.ordA_l[j]] >= t0; c1 += q.qn[q.ordB_l[j]] >= t0; }
+                    else { c0 += q.otu[q.ordA_u[j]] <= t0; c1 += q.qn[q.ordB_u[j]] <= t0; }
+                }
+            }
+            for (int o = 16; o; o >>= 1) {
+                c0 += __shfl_xor_sync(0xffffffffu, c0, o);
+                c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+            }
+            if ((t & 31) == 0) { atomicAdd(&s_cnt[0], c0); atomicAdd(&s_cnt[1], c1); }
+        }
+        __syncthreads();
+        Plan pl;
+        pl.kind = kind; pl.upper = upper; pl.p = p;
+        pl.idx1 = pl.idx2 = pl.kA0 = pl.kB0 = 0;
+        pl.nA = pl.nB = 0;
+        {
+            const int c0 = s_cnt[0], c1 = s_cnt[1];
             if (kind == 0) {
-                if (!upper) { pl.idx1 = lower_count(q.qs, m, t0) - 1; pl.nB = pl.idx1 + 1; }
-                else { pl.idx1 = upper_count(q.qs, m, t0); pl.nB = m - pl.idx1; }
+                if (!upper) { pl.idx1 = c0 - 1; pl.nB = pl.idx1 + 1; }
+                else { pl.idx1 = c0; pl.nB = m - pl.idx1; }
             } else if (kind == 1) {
                 if (!upper) {
-                    pl.idx1 = lower_count(q.qs, m, t0) - 1;
-                    pl.idx2 = min(pl.idx1, lower_count(q.tlq, m, t0) - 1);
+                    pl.idx1 = c0 - 1;
+                    pl.idx2 = min(pl.idx1, c1 - 1);
                     pl.nA = pl.idx2 + 1;
                     pl.nB = pl.idx1 + 1;
                 } else {
-                    pl.idx1 = upper_count(q.qs, m, t0);
-                    pl.idx2 = max(pl.idx1, upper_count(q.tuq, m, t0));
+                    pl.idx1 = c0;
+                    pl.idx2 = max(pl.idx1, c1);
                     pl.nA = m - pl.idx2;
                     pl.nB = m - pl.idx1;
                 }
             } else {
-                if (!upper) {
-                    const int* oa = q.ordA_l;
-                    const int* ob = q.ordB_l;
-                    pl.kA0 = prefix_count(m, [&](int k) { return q.otl[oa[k]] >= t0; });
-                    pl.kB0 = prefix_count(m, [&](int k) { return q.qn[ob[k]] >= t0; });
-                } else {
-                    const int* oa = q.ordA_u;
-                    const int* ob = q.ordB_u;
-                    pl.kA0 = prefix_count(m, [&](int k) { return q.otu[oa[k]] <= t0; });
-                    pl.kB0 = prefix_count(m, [&](int k) { return q.qn[ob[k]] <= t0; });
-                }
+                pl.kA0 = c0;
+                pl.kB0 = c1;
                 pl.nA = m - pl.kA0;
                 pl.nB = m - pl.kB0;
             }
-            s_plan = pl;
-            s_t0 = t0;
         }
-        __syncthreads();
-        const Plan pl = s_plan;
-        const double t0 = s_t0;
 
         // ---- 5. firing step of every op
         for (int r = t; r < pl.nA; r += T) {
@@ -383,59 +381,89 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
         __syncthreads();
         const int nops = s_nops;
 
-        // ---- 7. replay: initial sums then every op, in the reference's order
+        // ---- 7. replay: initial sums then every op, in the reference's order.
+        // The operands are gathered into shared memory by every thread first,
+        // so the one replaying thread only reads shared memory.
+        const double* pw0 = (kind == 2) ? q.opw : q.pw;
+        const double* Dt = (kind == 2) ? q.oD : q.Dq;
+        int* icode = sA;  // kind 2: per query element, 0 skip, 1 power sums, 2 penalty
+        for (int j = t; j < m; j += T) {
+            double* o = st + 4 * j;
+            o[0] = pw0[j]; o[1] = pw0[m + j]; o[2] = pw0[2 * m + j]; o[3] = Dt[j];
+            if (kind == 2) {
+                const double qv = q.qn[j];
+                int cd;
+                if (!upper) cd = (qv >= t0) ? 0 : (q.otl[j] >= t0 ? 1 : 2);
+                else cd = (qv <= t0) ? 0 : (q.otu[j] <= t0 ? 1 : 2);
+                icode[j] = cd;
+            }
+        }
+        __syncthreads();
         if (t == 0) {
             double mp0 = 0.0, mp1 = 0.0, mp2 = 0.0, C = 0.0;
-            const double* pw0 = (kind == 2) ? q.opw : q.pw;
-            const double* pw1 = pw0 + m;
-            const double* pw2 = pw0 + 2 * m;
+#define FSM_ADD_PW(j) { const double* o_ = st + 4 * (j); mp0 = dadd(mp0, o_[0]); mp1 = dadd(mp1, o_[1]); mp2 = dadd(mp2, o_[2]); }
             if (kind == 0) {
-                if (!upper) { for (int j = 0; j <= pl.idx1; ++j) { mp0 = dadd(mp0, pw0[j]); mp1 = dadd(mp1, pw1[j]); mp2 = dadd(mp2, pw2[j]); } }
-                else { for (int j = pl.idx1; j < m; ++j) { mp0 = dadd(mp0, pw0[j]); mp1 = dadd(mp1, pw1[j]); mp2 = dadd(mp2, pw2[j]); } }
+                if (!upper) { for (int j = 0; j <= pl.idx1; ++j) FSM_ADD_PW(j) }
+                else { for (int j = pl.idx1; j < m; ++j) FSM_ADD_PW(j) }
             } else if (kind == 1) {
                 if (!upper) {
-                    for (int j = pl.idx1; j > pl.idx2; --j) { mp0 = dadd(mp0, pw0[j]); mp1 = dadd(mp1, pw1[j]); mp2 = dadd(mp2, pw2[j]); }
-                    for (int j = 0; j <= pl.idx2; ++j) C = dadd(C, q.Dq[j]);
+                    for (int j = pl.idx1; j > pl.idx2; --j) FSM_ADD_PW(j)
+                    for (int j = 0; j <= pl.idx2; ++j) C = dadd(C, st[4 * j + 3]);
                 } else {
-                    for (int j = pl.idx1; j < pl.idx2; ++j) { mp0 = dadd(mp0, pw0[j]); mp1 = dadd(mp1, pw1[j]); mp2 = dadd(mp2, pw2[j]); }
-                    for (int j = pl.idx2; j < m; ++j) C = dadd(C, q.Dq[j]);
+                    for (int j = pl.idx1; j < pl.idx2; ++j) FSM_ADD_PW(j)
+                    for (int j = pl.idx2; j < m; ++j) C = dadd(C, st[4 * j + 3]);
                 }
             } else {
                 for (int e = 0; e < m; ++e) {
-                    const double qv = q.qn[e];
-                    if (!upper) {
-                        if (qv >= t0) continue;
-                        if (q.otl[e] >= t0) { mp0 = dadd(mp0, pw0[e]); mp1 = dadd(mp1, pw1[e]); mp2 = dadd(mp2, pw2[e]); }
-                        else C = dadd(C, q.oD[e]);
-                    } else {
-                        if (qv <= t0) continue;
-                        if (q.otu[e] <= t0) { mp0 = dadd(mp0, pw0[e]); mp1 = dadd(mp1, pw1[e]); mp2 = dadd(mp2, pw2[e]); }
-                        else C = dadd(C, q.oD[e]);
-                    }
+                    const int cd = icode[e];
+                    if (cd == 1) FSM_ADD_PW(e)
+                    else if (cd == 2) C = dadd(C, st[4 * e + 3]);
                 }
             }
+#undef FSM_ADD_PW
+            s_init[0] = mp0; s_init[1] = mp1; s_init[2] = mp2; s_init[3] = C;
+        }
+        __syncthreads();
+        // op payloads into the state slots the replay overwrites
+        for (int k = t; k < nops; k += T) {
+            const int d = opdesc[k];
+            double* o = st + 4 * (k + 1);
+            if (d < 0) {  // unreachable when the op order is a permutation; keeps reads in bounds
+                o[0] = o[1] = o[2] = o[3] = 0.0;
+                continue;
+            }
+            const int r = d & 0x3fffffff;
+            int x;  // table index of the op's query element
+            if (kind == 2) x = (d & 0x40000000) ? (upper ? q.ordB_u : q.ordB_l)[pl.kB0 + r]
+                                                : (upper ? q.ordA_u : q.ordA_l)[pl.kA0 + r];
+            else if (d & 0x40000000) x = upper ? pl.idx1 + r : pl.idx1 - r;
+            else x = upper ? pl.idx2 + r : pl.idx2 - r;
+            x = min(max(x, 0), m - 1);
+            o[0] = pw0[x]; o[1] = pw0[m + x]; o[2] = pw0[2 * m + x]; o[3] = Dt[x];
+        }
+        __syncthreads();
+        if (t == 0) {
+            double mp0 = s_init[0], mp1 = s_init[1], mp2 = s_init[2], C = s_init[3];
             st[0] = mp0; st[1] = mp1; st[2] = mp2; st[3] = C;
-            for (int k = 0; k < nops; ++k) {
-                const int d = opdesc[k];
-                double* o = st + 4 * (k + 1);
-                if (d < 0) {  // unreachable when the op order is a permutation; keeps reads in bounds
-                    o[0] = mp0; o[1] = mp1; o[2] = mp2; o[3] = C;
-                    continue;
-                }
-                const int r = d & 0x3fffffff;
-                int x;  // table index of the op's query element
-                if (kind == 2) x = (d & 0x40000000) ? (upper ? q.ordB_u : q.ordB_l)[pl.kB0 + r]
-                                                    : (upper ? q.ordA_u : q.ordA_l)[pl.kA0 + r];
-                else if (d & 0x40000000) x = upper ? pl.idx1 + r : pl.idx1 - r;
-                else x = upper ? pl.idx2 + r : pl.idx2 - r;
-                x = min(max(x, 0), m - 1);
-                if (d & 0x40000000) {
-                    mp0 = dsub(mp0, pw0[x]); mp1 = dsub(mp1, pw1[x]); mp2 = dsub(mp2, pw2[x]);
-                } else {
-                    C = dsub(C, (kind == 2) ? q.oD[x] : q.Dq[x]);
-                    mp0 = dadd(mp0, pw0[x]); mp1 = dadd(mp1, pw1[x]); mp2 = dadd(mp2, pw2[x]);
+            double* o = st + 4;
+            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+            int d = 0;
+            if (nops > 0) { a0 = o[0]; a1 = o[1]; a2 = o[2]; a3 = o[3]; d = opdesc[0]; }
+            for (int k = 0; k < nops; ++k, o += 4) {
+                // next op's operands before this op's state overwrites its slot
+                double n0 = 0.0, n1 = 0.0, n2 = 0.0, n3 = 0.0;
+                int nd = 0;
+                if (k + 1 < nops) { n0 = o[4]; n1 = o[5]; n2 = o[6]; n3 = o[7]; nd = opdesc[k + 1]; }
+                if (d >= 0) {
+                    if (d & 0x40000000) {
+                        mp0 = dsub(mp0, a0); mp1 = dsub(mp1, a1); mp2 = dsub(mp2, a2);
+                    } else {
+                        C = dsub(C, a3);
+                        mp0 = dadd(mp0, a0); mp1 = dadd(mp1, a1); mp2 = dadd(mp2, a2);
+                    }
                 }
                 o[0] = mp0; o[1] = mp1; o[2] = mp2; o[3] = C;
+                a0 = n0; a1 = n1; a2 = n2; a3 = n3; d = nd;
             }
         }
         __syncthreads();
@@ -470,14 +498,15 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
 
 size_t threshold_work_bytes(int cap_items, size_t sort_tmp, int m) {
     const size_t cap = (size_t)cap_items;
-    size_t x = ((sort_tmp > cap * 16 + 16 ? sort_tmp : cap * 16 + 16) + 15) & ~size_t(15);
-    size_t z = (size_t)m * 4 * 6 + 16 + (size_t)(2 * m + 1) * 4 * 8;
-    return x + z + 64;
+    const size_t runs = (cap * 12 + 4 + 15) & ~size_t(15);
+    const size_t x = ((sort_tmp > cap * 12 + 16 ? sort_tmp : cap * 12 + 16) + 15) & ~size_t(15);
+    const size_t z = (size_t)m * 4 * 6 + 16 + (size_t)(2 * m + 1) * 4 * 8;
+    return runs + x + z + 64;
 }
 
 template <int T, int IPT>
 size_t threshold_sort_tmp_bytes() {
-    return sizeof(typename cub::BlockMergeSort<RunKey, T, IPT>::TempStorage);
+    return sizeof(typename cub::BlockRadixSort<unsigned long long, T, IPT, int>::TempStorage);
 }
 
 #define FSM_THR_INST(T, IPT)                                                              \
