@@ -79,36 +79,22 @@ __device__ __forceinline__ bool lbip_exceeds(double bound, double cutoff, int me
     return true;
 }
 
-// Envelope of a z-normalised candidate window at point k (radius w, clipped to
-// the window [0, m)), from the raw target: x -> (x - mu) / sigma is monotone,
-// so min/max commute with it exactly.  tp, lraw, uraw point at the window start.
-__device__ __forceinline__ void cand_env(int k, int m, int w, const double* tp, const double* lraw,
-                                         const double* uraw, double mu, double sg, double* lo, double* up) {
-    double a, b;
-    if (k >= w && k <= m - 1 - w) {
-        a = lraw[k];
-        b = uraw[k];
-    } else {
-        const int s = k - w < 0 ? 0 : k - w, e = k + w > m - 1 ? m - 1 : k + w;
-        a = tp[s];
-        b = a;
-        for (int i = s + 1; i <= e; ++i) {
-            const double v = tp[i];
-            a = fmin(a, v);
-            b = fmax(b, v);
-        }
-    }
-    *lo = ddiv(dsub(a, mu), sg);
-    *up = ddiv(dsub(b, mu), sg);
-}
-
 // Q->T term of query point x (index k) against the candidate envelope: the
 // per-point term of src/glb.cpp:306-372; LCSS returns the match indicator.
-__device__ __forceinline__ double qt_term(int metric, double x, int k, int m, int w, const double* tp,
-                                          const double* lraw, const double* uraw, double mu, double sg,
-                                          double arg) {
-    double lo, up;
-    cand_env(k, m, w, tp, lraw, uraw, mu, sg, &lo, &up);
+// The candidate envelope at k is the min/max of the z-normalised window over
+// [max(0, k-w), min(m-1, k+w)] (lower_upper_lemire, src/glb.cpp:302-304).
+// x -> (x - mu) / sigma is monotone, so min/max commute with it exactly and
+// the raw min/max suffice.  lf/uf hold the target's forward windows
+// min/max(t[p .. p+w]) from the candidate start: the two windows starting at
+// p0 = max(0, k-w) and p1 = min(k, m-1-w) lie inside the candidate window and
+// their union is exactly [max(0, k-w), min(m-1, k+w)], so every point, edge
+// or interior, costs the same two reads per side.
+__device__ __forceinline__ double qt_term(int metric, double x, int k, int m, int w, const double* lf,
+                                          const double* uf, double mu, double sg, double arg) {
+    const int p0 = k - w < 0 ? 0 : k - w;
+    const int p1 = k < m - 1 - w ? k : m - 1 - w;
+    const double lo = ddiv(dsub(fmin(lf[p0], lf[p1]), mu), sg);
+    const double up = ddiv(dsub(fmax(uf[p0], uf[p1]), mu), sg);
     switch (metric) {
         case DTW:
             if (x < lo) return dsq(x, lo);

@@ -341,7 +341,7 @@ struct Stats {
     double* SIG = nullptr;
     double* Un = nullptr;
     double* Ln = nullptr;
-    double* Lraw = nullptr;  // centred radius-w min / max of the raw target
+    double* Lraw = nullptr;  // forward windows min / max(t[p .. p+w]) of the raw target
     double* Uraw = nullptr;
 };
 
@@ -389,7 +389,7 @@ static int run_env(fsmeld_ctx* c, const Geom& g, int w, Stats* st, const std::st
     if ((r = bufT(c, "lraw" + tag, (size_t)g.n, &st->Lraw))) return r;
     if ((r = bufT(c, "uraw" + tag, (size_t)g.n, &st->Uraw))) return r;
     prof_begin(c, ST_ENV);
-    k_raw_env<<<(unsigned)std::min<long long>((g.n + 255) / 256, (long long)c->sm_count * 32), 256, 0, c->stream>>>(
+    k_fwd_env<<<(unsigned)std::min<long long>((g.n + 255) / 256, (long long)c->sm_count * 32), 256, 0, c->stream>>>(
         c->d_target, g.n, w, st->Lraw, st->Uraw);
     LAUNCH_CHECK(c);
     const int mk = g.m_k;

@@ -109,19 +109,25 @@ __device__ __forceinline__ double dp_row(double* __restrict__ A, const double* _
             v = fmin3(dadd(pn, 1.0), dadd(left, 1.0), dadd(pd, sub));
             if (EXACT && d == d0) v = (double)rc.i;              // cur[0] = i
         } else if (METRIC == LCSS) {
-            double best = (fabs(dsub(xi, y)) <= arg) ? dadd(pd, 1.0) : pd;
-            if (best < pn) best = pn;
-            if (best < left) best = left;
+            // both sides computed, then selected: data-dependent branches here
+            // would split the warp cell by cell
+            const double hit1 = dadd(pd, 1.0);
+            double best = (fabs(dsub(xi, y)) <= arg) ? hit1 : pd;
+            best = (best < pn) ? pn : best;
+            best = (best < left) ? left : best;
             v = best;
-        } else {  // MSM, y = y_j, yprev = y_{j-1}
+        } else {  // MSM, y = y_j, yprev = y_{j-1}; every term computed, then selected
             const double axy = fabs(dsub(xi, y));
             const double c1 = dadd(pd, axy);
+            const bool xle = xi <= y, yle = y <= xi;
             // C(x_i, x_{i-1}, y_j): x_i lies between x_{i-1} and y_j
-            const bool b2 = (ge && xi <= y) || (y <= xi && le);
-            const double c2 = dadd(pn, b2 ? arg : dadd(arg, fmin(rc.c0, axy)));
+            const bool b2 = (ge && xle) || (yle && le);
+            const double m2 = dadd(arg, fmin(rc.c0, axy));
+            const double c2 = dadd(pn, b2 ? arg : m2);
             // C(y_j, x_i, y_{j-1}): y_j lies between x_i and y_{j-1}
-            const bool b3 = (xi <= y && y <= yprev) || (yprev <= y && y <= xi);
-            const double c3 = dadd(left, b3 ? arg : dadd(arg, fmin(axy, fabs(dsub(y, yprev)))));
+            const bool b3 = (xle && y <= yprev) || (yprev <= y && yle);
+            const double m3 = dadd(arg, fmin(axy, fabs(dsub(y, yprev))));
+            const double c3 = dadd(left, b3 ? arg : m3);
             v = fmin3(c1, c2, c3);
             if (EXACT && d == d0) v = dadd(pn, msm_c(xi, rc.xp, y, arg));  // column 0
             yprev = y;
@@ -303,7 +309,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
         }
         // cascading-bound term of this row's query point
         const bool use_term = has_s && (METRIC == LCSS || (k >= 1 && k <= m - 2));
-        const double term = use_term ? qt_term(METRIC, rc.xi, k, m, w, tp, lr, ur, mu, sg, arg) : 0.0;
+        const double term = use_term ? qt_term(METRIC, rc.xi, k, m, w, lr, ur, mu, sg, arg) : 0.0;
         double ext;
         if (!exact) {
             ext = dp_row<METRIC, false>(A, R, RM, W2, s0, rc, arg, 0, 0, -1);

@@ -9,9 +9,8 @@
 //    z-normalised window, src/glb.cpp:302-304) is never materialised:
 //    z-normalisation x -> (x - mu) / sigma is monotone even after rounding,
 //    so the minimum of the normalised points equals the normalised minimum of
-//    the raw points, bit for bit; interior envelope points come from a
-//    precomputed raw envelope of the target (k_raw_env) and only the 2w
-//    clipped edge windows are scanned.
+//    the raw points, bit for bit; every envelope point, edge or interior, is
+//    the min/max of two forward windows of the target (k_fwd_env).
 // Early abandon compares a running sum of non-negative terms with the
 // cutoff; running sums never decrease, so testing the final sum once is the
 // same decision as testing after every term.
@@ -156,15 +155,15 @@ __global__ void __launch_bounds__(256) k_glb_tq(Geom g, GlbJob job) {
     }
 }
 
-// Centred radius-w min/max of the raw target (NaN ignored; only positions
-// inside valid windows are ever read back).
-__global__ void __launch_bounds__(256) k_raw_env(const double* __restrict__ t, long long n, int w,
+// Forward windows of the raw target: lo/up[p] = min/max(t[p .. min(n-1, p+w)])
+// (NaN ignored; only windows inside valid candidate windows are ever read).
+__global__ void __launch_bounds__(256) k_fwd_env(const double* __restrict__ t, long long n, int w,
                                                  double* __restrict__ lo, double* __restrict__ up) {
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n;
          p += (long long)gridDim.x * blockDim.x) {
-        const long long a = p - w < 0 ? 0 : p - w, b = p + w > n - 1 ? n - 1 : p + w;
-        double mn = t[a], mx = t[a];
-        for (long long i = a + 1; i <= b; ++i) {
+        const long long b = p + w > n - 1 ? n - 1 : p + w;
+        double mn = t[p], mx = t[p];
+        for (long long i = p + 1; i <= b; ++i) {
             const double v = t[i];
             mn = fmin(mn, v);
             mx = fmax(mx, v);
@@ -202,8 +201,7 @@ __global__ void __launch_bounds__(128) k_glb_qt(Geom g, GlbJob job) {
             const double mu = job.MU[s * g.kml + j], sg = job.SIG[s * g.kml + j];
             const int k0 = (metric == LCSS) ? 0 : 1, k1 = (metric == LCSS) ? m - 1 : m - 2;
             for (int k = k0; k <= k1; ++k)
-                qt = dadd(qt, qt_term(metric, Q[k], k, m, w, job.target + gi, job.lraw + gi, job.uraw + gi, mu,
-                                      sg, arg));
+                qt = dadd(qt, qt_term(metric, Q[k], k, m, w, job.lraw + gi, job.uraw + gi, mu, sg, arg));
             if (metric == LCSS) {
                 glb = dmax0(dsub(1.0, ddiv(dminv(tq, qt), (double)m)));
             } else {

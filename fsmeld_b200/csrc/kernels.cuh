@@ -31,7 +31,7 @@ struct LbJob {
 struct GlbJob {
     QueryDev q;
     const double* target;
-    const double* lraw;         // centred radius-w min / max of the raw target
+    const double* lraw;         // forward windows min / max(t[p .. p+w]) of the raw target
     const double* uraw;
     const double* MU;
     const double* SIG;
@@ -51,7 +51,7 @@ struct GlbJob {
 struct DpJob {
     QueryDev q;
     const double* target;
-    const double* lraw;         // raw target envelope (cascading abandon terms)
+    const double* lraw;         // forward windows of the raw target (cascading abandon terms)
     const double* uraw;
     const double* MU;
     const double* SIG;
@@ -85,7 +85,7 @@ template <int T>
 __global__ void k_lbip(Geom g, LbJob job, const double2* __restrict__ W, int P, int logP);
 __global__ void k_glb_tq(Geom g, GlbJob job);
 __global__ void k_glb_qt(Geom g, GlbJob job);
-__global__ void k_raw_env(const double* __restrict__ t, long long n, int w, double* __restrict__ lo,
+__global__ void k_fwd_env(const double* __restrict__ t, long long n, int w, double* __restrict__ lo,
                           double* __restrict__ up);
 template <int METRIC>
 __global__ void k_dp(Geom g, DpJob job);
