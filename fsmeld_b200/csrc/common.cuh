@@ -48,13 +48,19 @@ struct Geom {
     long long forsize, S;  // full segments; total segments including the tail
     long long tsn;         // n - m + 1 windows
     long long excl_b, excl_e;
+    double inv_kml;        // fl(1 / kml), for the quotient estimate in locate()
     __host__ __device__ long long off(long long s) const { return s < forsize ? s * kml : n - m_k; }
     __host__ __device__ int lo(long long s) const { return s < forsize ? 0 : tail_lo; }
     __host__ __device__ long long gidx(long long s, int j) const { return s * kml + (j - lo(s)); }
     // statistics row/column of global window g
     __host__ __device__ void locate(long long g, long long* s, int* j) const {
-        long long q = g / kml;
-        if (q < forsize) { *s = q; *j = (int)(g - q * kml); }
+        // g / kml without a 64-bit integer division: the double estimate is
+        // within one of the quotient for g < 2^52; one step corrects it
+        long long q = (long long)((double)g * inv_kml);
+        long long r = g - q * kml;
+        if (r < 0) { --q; r += kml; }
+        else if (r >= kml) { ++q; r -= kml; }
+        if (q < forsize) { *s = q; *j = (int)r; }
         else { *s = forsize; *j = tail_lo + (int)(g - forsize * kml); }
     }
     __host__ __device__ bool excluded(long long g) const {

@@ -66,6 +66,7 @@ int make_geom(long long n, int m, long long eb, long long ee, Geom* g) {
     g->m = m;
     g->m_k = mk;
     g->kml = mk - m + 1;
+    g->inv_kml = 1.0 / (double)g->kml;
     g->tsn = n - m + 1;
     g->forsize = g->tsn / g->kml;
     const long long tail = g->tsn % g->kml;

@@ -28,8 +28,12 @@
 //    column formula, so sentinels are read exactly where the reference reads
 //    them whatever the magnitudes.
 //
-// DTW/LCSS start from a virtual cell (-1,-1) of value 0, which makes cell
-// (0,0) its own point distance (or match).
+// DTW/LCSS, and MSM in the fast mode, start from a virtual cell (-1,-1) of
+// value 0 above a row of sentinels: cell (0,0) becomes its own point distance
+// (or match), and MSM's row-0 cells j >= 1 keep only their left term,
+// cost[0][j-1] + C(y_j, x_0, y_{j-1}), the reference's row-0 loop
+// (src/ElasticMeasures.cpp:182-184).  A fresh candidate's band, ring padding
+// and first w+1 points are written by the whole warp, one pass each.
 //
 // Lanes are independent: each lane advances its own candidate one row per
 // step and, when its candidate finishes, takes the next one from a global
@@ -205,7 +209,8 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
         }
     };
 
-    // band before the first general row (the reference's initialisation loops)
+    // band before the first general row (the reference's initialisation
+    // loops), one lane alone: the restart of a candidate in the exact mode
     auto start = [&]() {
         ny = 0;
         over = false;
@@ -260,6 +265,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
             if (lane == leader) base = atomicAdd(job.next, (unsigned long long)__popc(need));
             base = __shfl_sync(0xffffffffu, base, leader);
             if (base >= n) { drained = true; break; }
+            bool fresh = false;
             if (!active) {
                 const unsigned long long c = base + __popc(need & ((1u << lane) - 1));
                 if (c < n) {
@@ -276,9 +282,68 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
                         has_s = job.list_s && job.lraw && job.list_s[c] >= 0.0;
                         Ssum = has_s ? job.list_s[c] : 0.0;
                         exact = query_exact;
-                        start();
+                        fresh = true;
                         active = true;
                     }
+                }
+            }
+            // The warp initialises each fresh lane's band, ring padding and
+            // first w+1 candidate points together, one pass each, instead of
+            // the fresh lane alone while the others wait.
+            unsigned fm = __ballot_sync(0xffffffffu, fresh);
+            while (fm) {
+                const int L = __ffs(fm) - 1;
+                fm &= fm - 1;
+                const double* tpL = (const double*)__shfl_sync(0xffffffffu, (unsigned long long)tp, L);
+                const double muL = __shfl_sync(0xffffffffu, mu, L);
+                const double sgL = __shfl_sync(0xffffffffu, sg, L);
+                double* AL = wbase + L;
+                double* RL = wbase + (size_t)(W2 + 1) * 32 + L;
+                for (int d = lane; d <= W2; d += 32) {
+                    double v = SENT;
+                    if (METRIC == EDR) {  // prev[j] = j, j <= min(m, w)
+                        if (d >= w && d - w <= min(m, w)) v = (double)(d - w);
+                    } else if (d == w) {  // DTW/LCSS/MSM: virtual (-1,-1) = 0; ERP: prev[0] = 0
+                        v = 0.0;
+                    }
+                    AL[d * 32] = v;
+                }
+                for (int c = lane; c <= w; c += 32) RL[((c - w - 1) & RM) * 32] = -kPad;  // left of the matrix
+                bool bad = false;
+                for (int c = lane; c <= w; c += 32) {
+                    double y = kPad;
+                    if (c < m) {
+                        y = ddiv(dsub(tpL[c], muL), sgL);
+                        bad = bad || !(fabs(y) <= ylim);
+                    }
+                    RL[(c & RM) * 32] = y;
+                }
+                const bool anybad = __any_sync(0xffffffffu, bad);
+                if (lane == L) over = anybad;
+            }
+            __syncwarp();
+            if (fresh) {
+                ny = w + 1;
+                Pre = 0.0;
+                row = ONE_BASED ? 1 : 0;
+                if (METRIC == ERP) {  // prev[j] = prev[j-1] + dist(y[j-1], g), j <= min(m, w)
+                    double acc = 0.0;
+                    for (int j = 1; j <= min(m, w); ++j) {
+                        acc = dadd(acc, dsq(R[((j - 1) & RM) * 32], arg));
+                        A[(j + w) * 32] = acc;
+                    }
+                }
+                if (METRIC == MSM && exact) {
+                    // exact mode: the reference's row 0, cost[0] = |x0-y0|,
+                    // cost[j] = cost[j-1] + C(y_j, x_0, y_{j-1}); the fast mode
+                    // computes row 0 as a general row from the virtual cell
+                    double acc = fabs(dsub(X[0], R[0]));
+                    A[w * 32] = acc;
+                    for (int j = 1; j < m && j <= w; ++j) {
+                        acc = dadd(acc, msm_c(R[(j & RM) * 32], X[0], R[((j - 1) & RM) * 32], arg));
+                        A[(j + w) * 32] = acc;
+                    }
+                    row = 1;
                 }
             }
         }
@@ -304,8 +369,16 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
         rc.i = i;
         if (METRIC == ERP) rc.c0 = dsq(rc.xi, arg);
         if (METRIC == MSM) {
-            rc.xp = X[i - 1];
-            rc.c0 = fabs(dsub(rc.xi, rc.xp));
+            if (i > 0) {
+                rc.xp = X[i - 1];
+                rc.c0 = fabs(dsub(rc.xi, rc.xp));
+            } else {
+                // row 0 (fast mode): with x_{-1} = -1e300 a move from the row
+                // above costs ~1e300 next to the left padding, so the virtual
+                // cell (-1,-1) reaches cell (0,0) only, through the diagonal
+                rc.xp = -kPad;
+                rc.c0 = kPad;
+            }
         }
         // cascading-bound term of this row's query point
         const bool use_term = has_s && (METRIC == LCSS || (k >= 1 && k <= m - 2));

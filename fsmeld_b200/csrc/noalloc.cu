@@ -158,6 +158,7 @@ extern "C" int fsmeld_exact_noalloc(int device, const double* device_target, int
     g.m = m;
     g.m_k = macro_length(m, n);
     g.kml = g.m_k - m + 1;
+    g.inv_kml = 1.0 / (double)g.kml;
     g.tsn = n - m + 1;
     g.forsize = g.tsn / g.kml;
     const long long tail = g.tsn % g.kml;
