@@ -136,28 +136,62 @@ def load_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
 
 
-def roofline(stage, dominant, geom, peaks, n_queries):
-    """Algorithmic bytes per launch of the dominant kernel over its average launch time."""
-    name, (ms, launches) = dominant
+# FP64 operations the reference's recurrence evaluates per band cell
+# (src/ElasticMeasures.cpp): DTW dist (sub, mul) + min of three (2) + add;
+# ERP three candidates of (sub, mul, add) + min of three; EDR sub, abs,
+# compare, three adds, min of three; LCSS sub, abs, compare, add, max of
+# three; MSM |x - y| + add, two split/merge costs (4 compares, 2 subs, 2 abs,
+# min, add) + adds, min of three.
+FLOPS_PER_CELL = {"dtw": 5, "erp": 11, "edr": 8, "lcss": 6, "msm": 27}
+# B200 FP64 issue rate: 148 SMs x 64 FP64 lanes x 1.965 GHz (the datasheet's
+# 37 TFLOP/s counts a fused multiply-add as two operations)
+FP64_PEAK_TOPS = 148 * 64 * 1.965e9 / 1e12
+
+
+def roofline(stages, cells, peaks):
+    """The dominant kernel, the exact DP (k_dp), is FP64-bound: algorithmic work
+    = band cells it computed (device counter; early abandon skips the rest) x
+    FP64 operations per cell of the reference's recurrence, over its average
+    launch time."""
+    ms, launches = stages["k_dp"]
+    flops = sum(cells[mt] * FLOPS_PER_CELL[mt] for mt in cells)
+    launches = max(1, launches)
+    avg_s = ms / launches / 1e3
+    achieved = flops / launches / avg_s / 1e12
+    traffic = None
+    try:
+        with open(PROFILE_SUMMARY) as f:
+            traffic = json.load(f).get("k_dp", {}).get("bytes_per_launch")
+    except Exception:
+        pass
+    return {"bound": "fp64", "kernel": "k_dp", "achieved": round(achieved, 3), "peak": round(FP64_PEAK_TOPS, 2),
+            "unit": "TFLOP/s", "frac": round(achieved / FP64_PEAK_TOPS, 4), "traffic": traffic,
+            "algorithmic_flops_per_launch": flops / launches, "avg_launch_ms": round(avg_s * 1e3, 4),
+            "dp_cells_per_launch": sum(cells.values()) / launches, "flops_per_cell": FLOPS_PER_CELL,
+            "peak_source": "nominal FP64 issue rate of B200 (148 SMs x 64 lanes x 1.965 GHz); "
+                           "MEASURED_PEAKS.json holds no FP64 figure"}
+
+
+def roofline_hbm(stages, geom, peaks):
+    """The window-statistics scan (k_mvmean), HBM-bound: reads every macro
+    segment's m_k target points once (the m-1 halo included) and writes mean and
+    sigma of its k_m_l windows."""
+    ms, launches = stages["k_mvmean"]
+    launches = max(1, launches)
     S, m_k, kml = geom["S"], geom["m_k"], geom["kml"]
-    # units per launch: one launch covers all S macro segments of one query (or, for the
-    # statistics, all segments shared by the batch).  Per segment the LB_IP path must read
-    # its m_k target points once (8 B each: the target plus the m-1 halo) -- 8*n*(1+(m-1)/kml)
-    # per query -- and write a survivor bitmask of kml/8 bytes.
-    bytes_per_launch = 8.0 * S * m_k + S * kml / 8.0
-    avg_s = ms / max(1, launches) / 1e3
+    bytes_per_launch = 8.0 * S * m_k + 16.0 * S * kml
+    avg_s = ms / launches / 1e3
     achieved = bytes_per_launch / avg_s / 1e9
     traffic = None
     try:
         with open(PROFILE_SUMMARY) as f:
-            tr = json.load(f)
-        traffic = tr.get(name, {}).get("bytes_per_launch")
+            traffic = json.load(f).get("k_mvmean", {}).get("bytes_per_launch")
     except Exception:
         pass
-    return {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
+    return {"bound": "hbm", "kernel": "k_mvmean", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
             "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
             "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": round(avg_s * 1e3, 4),
-            "peak_source": peaks["source"] + " (MEASURED_PEAKS.json hbm_gbs)" if peaks["source"] == "measured"
+            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks["source"] == "measured"
             else "fallback 6.65 TB/s"}
 
 
@@ -302,7 +336,7 @@ def impl_ours(args):
     geom = geometry(len(target), M)
     eng = api.Engine(target, device=local)
     metrics = [(mt, ag) for mt, ag in METRICS if args.case in (None, mt)]
-    if args.case or args.n_points != N_POINTS:
+    if args.case or args.fixed_cutoffs or args.n_points != N_POINTS:
         cutoffs = dict(CUTOFFS)  # profiling cases: the workload's constants, no setup launches
         cutoffs_match = None
     else:
@@ -329,11 +363,14 @@ def impl_ours(args):
     launches0 = eng.launches
     dev_ms = 0.0
     cand = 0
+    cells = {mt: 0 for mt, _ in metrics}
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             res = step()
             dev_ms += eng.last_call_ms
             cand += sum(r["counters"]["valid"] for r in res)
+            for (mt, _), r in zip(metrics, res):
+                cells[mt] += r["counters"]["dp_cells"]
     torch.cuda.synchronize()
     launches = eng.launches - launches0
     stages = eng.stage_times()
@@ -371,7 +408,6 @@ def impl_ours(args):
 
     if rank == 0:
         peaks = load_peaks()
-        dominant = max(stages.items(), key=lambda kv: kv[1][0])
         line = {
             "metric": "candidates/s", "value": value, "unit": "candidates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max_ms / args.steps,
@@ -384,7 +420,9 @@ def impl_ours(args):
                        "l2": "inputs larger than L2 (134 MB target per GPU)",
                        "cutoffs": cutoffs, "cutoffs_match_workload_constants": cutoffs_match},
             "queries_per_s": len(metrics) * world / (t_max_ms / 1e3 / args.steps),
-            "roofline": roofline(stages, dominant, geom, peaks, len(metrics)),
+            "roofline": roofline(stages, cells, peaks),
+            "roofline_hbm": roofline_hbm(stages, geom, peaks),
+            "dominant_kernel": max(stages.items(), key=lambda kv: kv[1][0])[0],
             "stage_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in stages.items()},
             "e2e": {"value": e2e_value, "unit": "candidates/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -411,6 +449,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--case", choices=[m for m, _ in METRICS], help="one metric's query only (profiling runs)")
     ap.add_argument("--n-points", type=int, default=N_POINTS, help="target length (profiling runs)")
+    ap.add_argument("--fixed-cutoffs", action="store_true",
+                    help="use the workload's cutoff constants without recomputing them (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         return impl_reference(args)

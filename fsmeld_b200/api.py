@@ -38,7 +38,8 @@ class Counters(C.Structure):
     _fields_ = [("valid", C.c_int64), ("invalid", C.c_int64), ("after_lb", C.c_int64),
                 ("after_glb", C.c_int64), ("exact_evals", C.c_int64), ("matches", C.c_int64),
                 ("threshold", C.c_double), ("m_k", C.c_int32), ("reserved", C.c_int32),
-                ("segments", C.c_int64), ("tail", C.c_int64), ("device_ms", C.c_double)]
+                ("segments", C.c_int64), ("tail", C.c_int64), ("device_ms", C.c_double),
+                ("dp_cells", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

@@ -477,7 +477,7 @@ static int run_lbip(fsmeld_ctx* c, const Geom& g, LbJob job) {
 }
 
 // counters slot layout
-enum { C_SURV, C_G1, C_G2, C_OUT, C_VALID, C_SEED, C_SEEDOUT, C_DPNEXT, C_N };
+enum { C_SURV, C_G1, C_G2, C_OUT, C_VALID, C_SEED, C_SEEDOUT, C_DPNEXT, C_CELLS, C_N };
 
 static int run_glb(fsmeld_ctx* c, const Geom& g, const QueryDev& qd, const Stats& st, const long long* in,
                    unsigned long long* cnt, long long cap, long long* segc, long long** out_list,
@@ -648,7 +648,7 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
         DpJob dj{};
         dj.q = qd; dj.target = c->d_target; dj.MU = st.MU; dj.SIG = st.SIG;
         dj.list = nullptr; dj.n_windows = g.tsn; dj.mode = 0; dj.cutoff = qr.cutoff;
-        dj.out_idx = oi; dj.out_dist = od; dj.n_out = cnt + C_OUT; dj.out_cap = cap; dj.n_valid = cnt + C_VALID;
+        dj.out_idx = oi; dj.out_dist = od; dj.n_out = cnt + C_OUT; dj.n_cells = cnt + C_CELLS; dj.out_cap = cap; dj.n_valid = cnt + C_VALID;
         if ((r = run_dp(c, g, dj, g.tsn))) return r;
         FSM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
         FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -664,6 +664,7 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
         out.invalid = g.tsn - out.valid;
         out.after_lb = out.after_glb = out.exact_evals = out.valid;
         out.matches = nout;
+        out.dp_cells = (long long)h[C_CELLS];
         out.threshold = qr.cutoff;
         if (qr.out_count) *qr.out_count = nout;
         if (qr.cnt) *qr.cnt = out;
@@ -701,7 +702,7 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
         dj.q = qd; dj.target = c->d_target; dj.MU = st.MU; dj.SIG = st.SIG;
         dj.lraw = st.Lraw; dj.uraw = st.Uraw;
         dj.list = g2; dj.list_s = g2t; dj.n_list = cnt + C_G2; dj.list_cap = cap; dj.mode = 0; dj.cutoff = qr.cutoff;
-        dj.out_idx = oi; dj.out_dist = od; dj.n_out = cnt + C_OUT; dj.out_cap = cap; dj.n_valid = nullptr;
+        dj.out_idx = oi; dj.out_dist = od; dj.n_out = cnt + C_OUT; dj.n_cells = cnt + C_CELLS; dj.out_cap = cap; dj.n_valid = nullptr;
         if ((r = run_dp(c, g, dj, (long long)c->sm_count * 16 * 128))) return r;
         FSM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
         FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -720,6 +721,7 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
         out.after_glb = (long long)h[C_G2];
         out.exact_evals = out.after_glb;
         out.matches = nout;
+        out.dp_cells = (long long)h[C_CELLS];
         out.threshold = qr.cutoff;
         if (qr.out_count) *qr.out_count = nout;
         if (qr.cnt) *qr.cnt = out;
@@ -747,7 +749,7 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
     DpJob sj{};
     sj.q = qd; sj.target = c->d_target; sj.MU = st.MU; sj.SIG = st.SIG;
     sj.list = seeds; sj.n_list = cnt + C_SEED; sj.list_cap = g.S; sj.mode = 1; sj.cutoff = DBL_MAX;
-    sj.out_idx = si; sj.out_dist = sd; sj.n_out = cnt + C_SEEDOUT; sj.out_cap = g.S;
+    sj.out_idx = si; sj.out_dist = sd; sj.n_out = cnt + C_SEEDOUT; sj.n_cells = cnt + C_CELLS; sj.out_cap = g.S;
     if ((r = run_dp(c, g, sj, g.S))) return r;
     FSM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
     FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -781,7 +783,7 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
     dj.q = qt; dj.target = c->d_target; dj.MU = st.MU; dj.SIG = st.SIG;
     dj.lraw = st.Lraw; dj.uraw = st.Uraw;
     dj.list = g2; dj.list_s = g2t; dj.n_list = cnt + C_G2; dj.list_cap = cap; dj.mode = 1; dj.cutoff = tau;
-    dj.out_idx = oi; dj.out_dist = od; dj.n_out = cnt + C_OUT; dj.out_cap = cap;
+    dj.out_idx = oi; dj.out_dist = od; dj.n_out = cnt + C_OUT; dj.n_cells = cnt + C_CELLS; dj.out_cap = cap;
     if ((r = run_dp(c, g, dj, (long long)c->sm_count * 16 * 128))) return r;
     FSM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
     FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -799,6 +801,7 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
     out.after_glb = (long long)h[C_G2];
     out.exact_evals = (long long)h[C_G2] + nseed;
     out.matches = qr.k;
+    out.dp_cells = (long long)h[C_CELLS];
     out.threshold = kd[qr.k - 1];
     if (qr.out_count) *qr.out_count = qr.k;
     if (qr.cnt) *qr.cnt = out;

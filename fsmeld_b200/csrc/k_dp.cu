@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
         }
     };
 
-    unsigned long long valid_count = 0;
+    unsigned long long valid_count = 0, cells = 0;
     bool drained = false;
     for (;;) {
         // refill idle lanes from the work counter (lanes that draw an invalid
@@ -392,6 +392,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
             ext = dp_row<METRIC, true>(A, R, RM, W2, s0, rc, arg, dlo, dhi, d0);
         }
         if (use_term) Pre = dadd(Pre, term);
+        cells += (unsigned long long)W2;
 
         bool done = false, keep = false;
         double dist = 0.0;
@@ -428,6 +429,10 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
     if (job.n_valid) {
         for (int o = 16; o; o >>= 1) valid_count += __shfl_xor_sync(0xffffffffu, valid_count, o);
         if (lane == 0 && valid_count) atomicAdd(job.n_valid, valid_count);
+    }
+    if (job.n_cells) {
+        for (int o = 16; o; o >>= 1) cells += __shfl_xor_sync(0xffffffffu, cells, o);
+        if (lane == 0 && cells) atomicAdd(job.n_cells, cells);
     }
 }
 

@@ -70,6 +70,7 @@ struct DpJob {
     unsigned long long* next;   // work counter (zeroed before the launch)
     double* gwork;              // global band scratch when shared memory is too small
     int force_exact;            // every candidate in the DP's exact boundary mode
+    unsigned long long* n_cells;  // band cells computed (optional)
 };
 
 __global__ void k_mvmean(const double* __restrict__ target, Geom g, double* __restrict__ mu,

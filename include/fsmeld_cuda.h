@@ -64,6 +64,7 @@ typedef struct {
     int64_t segments;     /* full macro segments */
     int64_t tail;         /* windows in the EOF-aligned tail segment */
     double device_ms;     /* device time of the call (CUDA events) */
+    int64_t dp_cells;     /* band cells the exact DP computed (rows done x (2w+1)) */
 } fsmeld_counters;
 
 /* one query of a batched call */
