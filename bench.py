@@ -45,6 +45,7 @@ CUTOFFS = {"dtw": 2.80906383446946, "erp": 5.138604886191949, "edr": 48.0, "lcss
            "msm": 74.7957914893858}
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+LATENCY_REPS = 10  # plain single-query requests per query for the latency figures
 
 
 def log(*a):
@@ -404,6 +405,24 @@ def impl_ours(args):
             e2e_cand += sum(r["counters"]["valid"] for r in res)
             d2h = sum(int(r["count"]) * 8 + 96 for r in res)
     e2e_value = e2e_cand / e2e_secs * world if e2e_secs > 0 else None
+
+    # request latency: every query issued alone through the plain (unbatched)
+    # search call, device time per request; and the batched call's speed-up
+    # over issuing the same queries one by one
+    lat = []
+    for _ in range(0 if args.no_e2e else LATENCY_REPS):
+        for b in batch:
+            eng.search(b["query"], b["m"], b["cutoff"], b["metric"], b["w"], b["arg"])
+            lat.append(eng.last_call_ms)
+    latency = None
+    if lat:
+        lat_a = np.asarray(lat)
+        plain_ms = float(lat_a.sum()) / LATENCY_REPS
+        batched_ms = t_max_ms / args.steps
+        latency = {"requests": len(lat), "p50_ms": round(float(np.percentile(lat_a, 50)), 3),
+                   "p99_ms": round(float(np.percentile(lat_a, 99)), 3),
+                   "plain_ms_per_step": round(plain_ms, 3), "batched_ms_per_step": round(batched_ms, 3),
+                   "batched_speedup": round(plain_ms / batched_ms, 3)}
     h2d = len(target) * 8 + sum(M * 8 for _ in METRICS)
 
     if rank == 0:
@@ -426,6 +445,7 @@ def impl_ours(args):
             "stage_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in stages.items()},
             "e2e": {"value": e2e_value, "unit": "candidates/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
+            "latency": latency,
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
