@@ -95,12 +95,14 @@ __device__ __forceinline__ bool lbip_exceeds(double bound, double cutoff, int me
 // p0 = max(0, k-w) and p1 = min(k, m-1-w) lie inside the candidate window and
 // their union is exactly [max(0, k-w), min(m-1, k+w)], so every point, edge
 // or interior, costs the same two reads per side.
-__device__ __forceinline__ double qt_term(int metric, double x, int k, int m, int w, const double* lf,
-                                          const double* uf, double mu, double sg, double arg) {
-    const int p0 = k - w < 0 ? 0 : k - w;
-    const int p1 = k < m - 1 - w ? k : m - 1 - w;
-    const double lo = ddiv(dsub(fmin(lf[p0], lf[p1]), mu), sg);
-    const double up = ddiv(dsub(fmax(uf[p0], uf[p1]), mu), sg);
+__device__ __forceinline__ int qt_p0(int k, int w) { return k - w < 0 ? 0 : k - w; }
+__device__ __forceinline__ int qt_p1(int k, int m, int w) { return k < m - 1 - w ? k : m - 1 - w; }
+
+// The term from the raw window minimum a and maximum b of the candidate at k.
+__device__ __forceinline__ double qt_term_env(int metric, double x, double a, double b, double mu, double sg,
+                                              double arg) {
+    const double lo = ddiv(dsub(a, mu), sg);
+    const double up = ddiv(dsub(b, mu), sg);
     switch (metric) {
         case DTW:
             if (x < lo) return dsq(x, lo);
@@ -123,6 +125,12 @@ __device__ __forceinline__ double qt_term(int metric, double x, int k, int m, in
             if (x < lo) { const double p = fabs(dsub(x, lo)); return (p < arg) ? p : arg; }
             return 0.0;
     }
+}
+
+__device__ __forceinline__ double qt_term(int metric, double x, int k, int m, int w, const double* lf,
+                                          const double* uf, double mu, double sg, double arg) {
+    const int p0 = qt_p0(k, w), p1 = qt_p1(k, m, w);
+    return qt_term_env(metric, x, fmin(lf[p0], lf[p1]), fmax(uf[p0], uf[p1]), mu, sg, arg);
 }
 
 // Per-query tables prepared on the host (query z-normalisation as

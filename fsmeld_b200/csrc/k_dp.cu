@@ -59,8 +59,6 @@ namespace {
 
 constexpr double kPad = 1e300;  // candidate points outside the matrix (fast mode)
 
-__device__ __forceinline__ double fmin3(double a, double b, double c) { return fmin(fmin(a, b), c); }
-
 // Cascading abandon margin: the bound and the DP carry independent round-off
 // (relative ~1e-13); a 1e-9 relative slack keeps the test conservative.
 __device__ __forceinline__ double slack(double cut) { return cut + 1e-9 * (1.0 + fabs(cut)); }
@@ -77,70 +75,94 @@ struct RowCtx {
     double xi;   // query point of the row
     double c0;   // ERP: dist(x, g); MSM: |x_i - x_{i-1}|
     double xp;   // MSM: x_{i-1}
+    bool ge, le; // MSM: x_{i-1} <= x_i, x_i <= x_{i-1}
     int i;       // row
 };
+
+// Minimum / maximum by one comparison and a select.  Every DP value here is
+// a non-NaN number >= +0 (sums of non-negative terms, match counts, +inf at
+// most), so they equal std::min/std::max (and fmin/fmax) on these operands;
+// fmin/fmax also handle NaN operands, which costs extra instructions per call.
+__device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
+
+// One cell.  pn/pd: the previous row's cells above and diagonally left; left:
+// this row's previous cell; y: the candidate point read by the cell (y_j, or
+// y[j-1] for ERP/EDR); yprev: y_{j-1} (MSM).
+template <int METRIC, bool EXACT>
+__device__ __forceinline__ double dp_cell(double pn, double pd, double left, double y, double yprev,
+                                          const RowCtx& rc, double arg, int d, int dlo, int dhi, int d0) {
+    constexpr double SENT = (METRIC == LCSS) ? 0.0 : kDpMax;
+    const double xi = rc.xi;
+    double v;
+    // the minimum of three non-negative values does not depend on the order:
+    // the left neighbour (the previous cell of this row) enters last, so the
+    // chain from one cell to the next is one minimum and one add
+    if (METRIC == DTW) {
+        v = dadd(smin(smin(pn, pd), left), dsq(xi, y));
+    } else if (METRIC == ERP) {  // y = y[j-1]
+        const double match = dadd(pd, dsq(xi, y));
+        const double ins = dadd(left, dsq(y, arg));
+        const double del = dadd(pn, rc.c0);
+        v = smin(smin(match, del), ins);
+        if (EXACT && d == d0) v = del;                       // cur[0] = prev[0] + dist(x, g)
+    } else if (METRIC == EDR) {  // y = y[j-1]
+        const double sub = (fabs(dsub(xi, y)) <= arg) ? 0.0 : 1.0;
+        v = smin(smin(dadd(pn, 1.0), dadd(pd, sub)), dadd(left, 1.0));
+        if (EXACT && d == d0) v = (double)rc.i;              // cur[0] = i
+    } else if (METRIC == LCSS) {
+        // both sides computed, then selected: data-dependent branches here
+        // would split the warp cell by cell
+        const double hit1 = dadd(pd, 1.0);
+        double best = (fabs(dsub(xi, y)) <= arg) ? hit1 : pd;
+        best = (best < pn) ? pn : best;
+        best = (best < left) ? left : best;
+        v = best;
+    } else {  // MSM, y = y_j, yprev = y_{j-1}; every term computed, then selected
+        const double axy = fabs(dsub(xi, y));
+        const double c1 = dadd(pd, axy);
+        const bool xle = xi <= y, yle = y <= xi;
+        // C(x_i, x_{i-1}, y_j): x_i lies between x_{i-1} and y_j
+        const bool b2 = (rc.ge && xle) || (yle && rc.le);
+        const double m2 = dadd(arg, smin(rc.c0, axy));
+        const double c2 = dadd(pn, b2 ? arg : m2);
+        // C(y_j, x_i, y_{j-1}): y_j lies between x_i and y_{j-1}
+        const bool b3 = (xle && y <= yprev) || (yprev <= y && yle);
+        const double m3 = dadd(arg, smin(axy, fabs(dsub(y, yprev))));
+        const double c3 = dadd(left, b3 ? arg : m3);
+        v = smin(smin(c1, c2), c3);
+        if (EXACT && d == d0) v = dadd(pn, msm_c(xi, rc.xp, y, arg));  // column 0
+    }
+    if (EXACT && (d < dlo || d > dhi)) v = SENT;
+    return v;
+}
 
 // One band row in place.  A: band row [d * 32], A[W2 * 32] is a permanent
 // out-of-band cell; R: ring [slot * 32], RM = ring size - 1; s0: ring index
 // of the candidate column read by cell d = 0 (the column itself for
-// DTW/LCSS/MSM, column j-1 for ERP/EDR).  Returns the row minimum (maximum
-// for LCSS).  EXACT: clip cells outside [dlo, dhi] to the sentinel and use
-// the reference's column-0 formula (cell d0 = w - i).
+// DTW/LCSS/MSM, column j-1 for ERP/EDR).  One loop of 2w+1 cells with a
+// masked ring index: lanes sit at different rows, so a loop split where the
+// ring wraps would differ between lanes and run both parts for all of them.
+// Returns the row minimum (maximum for LCSS).  EXACT: clip cells outside
+// [dlo, dhi] to the sentinel and use the reference's column-0 formula (cell
+// d0 = w - i).
 template <int METRIC, bool EXACT>
 __device__ __forceinline__ double dp_row(double* __restrict__ A, const double* __restrict__ R, int RM, int W2,
                                          int s0, const RowCtx& rc, double arg, int dlo, int dhi, int d0) {
     constexpr double SENT = (METRIC == LCSS) ? 0.0 : kDpMax;
-    const double xi = rc.xi;
     double left = SENT, ext = SENT;
     double pd = A[0];
     double yprev = (METRIC == MSM) ? R[((s0 - 1) & RM) * 32] : 0.0;  // y_{j-1} for MSM
-    const bool ge = rc.xp <= xi, le = xi <= rc.xp;
 #pragma unroll 3
     for (int d = 0; d < W2; ++d) {
         const double pn = A[(d + 1) * 32];
         const double y = R[((s0 + d) & RM) * 32];
-        double v;
-        if (METRIC == DTW) {
-            v = dadd(fmin3(pn, left, pd), dsq(xi, y));
-        } else if (METRIC == ERP) {  // y = y[j-1]
-            const double match = dadd(pd, dsq(xi, y));
-            const double ins = dadd(left, dsq(y, arg));
-            const double del = dadd(pn, rc.c0);
-            v = fmin3(match, ins, del);
-            if (EXACT && d == d0) v = del;                       // cur[0] = prev[0] + dist(x, g)
-        } else if (METRIC == EDR) {  // y = y[j-1]
-            const double sub = (fabs(dsub(xi, y)) <= arg) ? 0.0 : 1.0;
-            v = fmin3(dadd(pn, 1.0), dadd(left, 1.0), dadd(pd, sub));
-            if (EXACT && d == d0) v = (double)rc.i;              // cur[0] = i
-        } else if (METRIC == LCSS) {
-            // both sides computed, then selected: data-dependent branches here
-            // would split the warp cell by cell
-            const double hit1 = dadd(pd, 1.0);
-            double best = (fabs(dsub(xi, y)) <= arg) ? hit1 : pd;
-            best = (best < pn) ? pn : best;
-            best = (best < left) ? left : best;
-            v = best;
-        } else {  // MSM, y = y_j, yprev = y_{j-1}; every term computed, then selected
-            const double axy = fabs(dsub(xi, y));
-            const double c1 = dadd(pd, axy);
-            const bool xle = xi <= y, yle = y <= xi;
-            // C(x_i, x_{i-1}, y_j): x_i lies between x_{i-1} and y_j
-            const bool b2 = (ge && xle) || (yle && le);
-            const double m2 = dadd(arg, fmin(rc.c0, axy));
-            const double c2 = dadd(pn, b2 ? arg : m2);
-            // C(y_j, x_i, y_{j-1}): y_j lies between x_i and y_{j-1}
-            const bool b3 = (xle && y <= yprev) || (yprev <= y && yle);
-            const double m3 = dadd(arg, fmin(axy, fabs(dsub(y, yprev))));
-            const double c3 = dadd(left, b3 ? arg : m3);
-            v = fmin3(c1, c2, c3);
-            if (EXACT && d == d0) v = dadd(pn, msm_c(xi, rc.xp, y, arg));  // column 0
-            yprev = y;
-        }
-        if (EXACT && (d < dlo || d > dhi)) v = SENT;
+        const double v = dp_cell<METRIC, EXACT>(pn, pd, left, y, yprev, rc, arg, d, dlo, dhi, d0);
         A[d * 32] = v;
         left = v;
         pd = pn;
-        ext = (METRIC == LCSS) ? fmax(ext, v) : fmin(ext, v);
+        yprev = y;
+        ext = (METRIC == LCSS) ? smax(ext, v) : smin(ext, v);
     }
     return ext;
 }
@@ -166,6 +188,13 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
         (job.list && n_all > (unsigned long long)job.list_cap) ? job.list_cap : n_all;
     const double cut = job.cutoff;
     const double arg = q.arg;
+    // abandon thresholds, once per kernel, each a little looser than the plain
+    // test so that it can only abandon less: DTW/ERP sqrt(b) > s as b > s^2,
+    // LCSS 1 - v/m > s as v < m(1 - s) (s = the slackened cutoff)
+    const double cut_s = slack(cut);
+    const bool neg_lim = cut_s < 0.0;
+    const double cut_sq = dmul(dmul(cut_s, cut_s), 1.0 + 0x1p-50);
+    const double lcss_lim = dmul(dmul((double)m, dsub(1.0, cut_s)), 1.0 - 0x1p-50);
     constexpr bool ONE_BASED = (METRIC == ERP || METRIC == EDR);  // rows 1..m, columns 0..m
     constexpr double SENT = (METRIC == LCSS) ? 0.0 : kDpMax;
     const int last = ONE_BASED ? m : m - 1;  // last row and last column
@@ -196,13 +225,29 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
     int row = 0, ny = 0;
     double Ssum = 0.0, Pre = 0.0;  // GLB Q->T sum of the candidate, and its prefix over rows done
     bool has_s = false;
+    // inputs of the lane's next row, loaded one row ahead so that their
+    // latency overlaps the current row: query points, the next raw candidate
+    // point (held for index nty) and the cascade term's forward-window reads
+    double nx = 0.0, nxp = 0.0, nt = 0.0, na0 = 0.0, na1 = 0.0, nb0 = 0.0, nb1 = 0.0;
+    int nty = -1;
+    auto prefetch = [&](int r) {
+        const int k = ONE_BASED ? r - 1 : r;
+        nx = X[k];
+        if (METRIC == MSM) nxp = (r > 0) ? X[r - 1] : -kPad;
+        if (ny < m) { nt = tp[ny]; nty = ny; }
+        if (has_s && (METRIC == LCSS || (k >= 1 && k <= m - 2))) {
+            const int p0 = qt_p0(k, w), p1 = qt_p1(k, m, w);
+            na0 = lr[p0]; na1 = lr[p1];
+            nb0 = ur[p0]; nb1 = ur[p1];
+        }
+    };
 
     // candidate points ny..upto into the ring; columns past the window are padding
     auto fill_ring = [&](int upto) {
         for (; ny <= upto; ++ny) {
             double y = kPad;
             if (ny < m) {
-                y = ddiv(dsub(tp[ny], mu), sg);
+                y = ddiv(dsub(ny == nty ? nt : tp[ny], mu), sg);
                 over = over || !(fabs(y) <= ylim);
             }
             R[(ny & RM) * 32] = y;
@@ -345,6 +390,8 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
                     }
                     row = 1;
                 }
+                nty = -1;
+                prefetch(row);
             }
         }
         if (!__any_sync(0xffffffffu, active)) {
@@ -358,31 +405,32 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
         fill_ring(s0 + 2 * w);                          // one new point per row in steady state
         if (over && !exact) {                           // out of the fast-mode range: restart exact
             exact = true;
+            nty = -1;
             start();
+            prefetch(row);
             continue;
         }
         const int k = ONE_BASED ? i - 1 : i;  // query index aligned by this row
         RowCtx rc;
-        rc.xi = X[k];
+        rc.xi = nx;
         rc.c0 = 0.0;
         rc.xp = rc.xi;
         rc.i = i;
         if (METRIC == ERP) rc.c0 = dsq(rc.xi, arg);
         if (METRIC == MSM) {
-            if (i > 0) {
-                rc.xp = X[i - 1];
-                rc.c0 = fabs(dsub(rc.xi, rc.xp));
-            } else {
-                // row 0 (fast mode): with x_{-1} = -1e300 a move from the row
-                // above costs ~1e300 next to the left padding, so the virtual
-                // cell (-1,-1) reaches cell (0,0) only, through the diagonal
-                rc.xp = -kPad;
-                rc.c0 = kPad;
-            }
+            // row 0 (fast mode): with x_{-1} = -1e300 a move from the row above
+            // costs ~1e300 next to the left padding, so the virtual cell
+            // (-1,-1) reaches cell (0,0) only, through the diagonal
+            rc.xp = (i > 0) ? nxp : -kPad;
+            rc.c0 = fabs(dsub(rc.xi, rc.xp));
         }
-        // cascading-bound term of this row's query point
+        rc.ge = rc.xp <= rc.xi;
+        rc.le = rc.xi <= rc.xp;
+        // cascading-bound term of this row's query point (inputs loaded a row ahead)
         const bool use_term = has_s && (METRIC == LCSS || (k >= 1 && k <= m - 2));
-        const double term = use_term ? qt_term(METRIC, rc.xi, k, m, w, lr, ur, mu, sg, arg) : 0.0;
+        const double ta = fmin(na0, na1), tb = fmax(nb0, nb1);
+        if (i < last) prefetch(i + 1);  // next row's loads overlap this row's cells
+        const double term = use_term ? qt_term_env(METRIC, rc.xi, ta, tb, mu, sg, arg) : 0.0;
         double ext;
         if (!exact) {
             ext = dp_row<METRIC, false>(A, R, RM, W2, s0, rc, arg, 0, 0, -1);
@@ -408,10 +456,14 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
             // query point meets the candidate envelope
             double rest = (double)(m - 1 - i);
             if (has_s) rest = fmin(rest, fmax(0.0, dsub(Ssum, Pre)));
-            if (dsub(1.0, ddiv(dadd(ext, rest), (double)m)) > slack(cut)) done = true;
+            if (dadd(ext, rest) < lcss_lim) done = true;
         } else {
             const double bnd = dadd(ext, fmax(0.0, dsub(Ssum, Pre)));
-            if ((METRIC == DTW || METRIC == ERP ? dsqrt(dmax0(bnd)) : bnd) > slack(cut)) done = true;
+            if (METRIC == DTW || METRIC == ERP) {
+                if (neg_lim || bnd > cut_sq) done = true;
+            } else if (bnd > cut_s) {
+                done = true;
+            }
         }
         if (done) {
             active = false;
