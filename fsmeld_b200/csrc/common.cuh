@@ -130,7 +130,9 @@ __device__ __forceinline__ double qt_term_env(int metric, double x, double a, do
 __device__ __forceinline__ double qt_term(int metric, double x, int k, int m, int w, const double* lf,
                                           const double* uf, double mu, double sg, double arg) {
     const int p0 = qt_p0(k, w), p1 = qt_p1(k, m, w);
-    return qt_term_env(metric, x, fmin(lf[p0], lf[p1]), fmax(uf[p0], uf[p1]), mu, sg, arg);
+    // valid windows hold no NaN: a comparison and a select give the min / max
+    const double a0 = lf[p0], a1 = lf[p1], b0 = uf[p0], b1 = uf[p1];
+    return qt_term_env(metric, x, (a1 < a0) ? a1 : a0, (b0 < b1) ? b1 : b0, mu, sg, arg);
 }
 
 // Per-query tables prepared on the host (query z-normalisation as

@@ -496,9 +496,19 @@ static int run_glb(fsmeld_ctx* c, const Geom& g, const QueryDev& qd, const Stats
     j1.out = g1; j1.out_b = g1b; j1.out_t = g1t; j1.n_out = cnt + C_G1; j1.out_cap = cap;
     j1.segc = segc;
     const size_t sm1 = sizeof(double) * 3 * qd.m;
-    if ((r = allow_smem(c, k_glb_tq, sm1))) return r;
+    const void* tqf = qd.metric == DTW ? (const void*)k_glb_tq<DTW>
+                    : qd.metric == ERP ? (const void*)k_glb_tq<ERP>
+                    : qd.metric == EDR ? (const void*)k_glb_tq<EDR>
+                    : qd.metric == LCSS ? (const void*)k_glb_tq<LCSS> : (const void*)k_glb_tq<MSM>;
+    if ((r = allow_smem(c, tqf, sm1))) return r;
     prof_begin(c, ST_GLB1);
-    k_glb_tq<<<c->sm_count * 8, 256, sm1, c->stream>>>(g, j1);
+    switch (qd.metric) {
+        case DTW: k_glb_tq<DTW><<<c->sm_count * 8, 256, sm1, c->stream>>>(g, j1); break;
+        case ERP: k_glb_tq<ERP><<<c->sm_count * 8, 256, sm1, c->stream>>>(g, j1); break;
+        case EDR: k_glb_tq<EDR><<<c->sm_count * 8, 256, sm1, c->stream>>>(g, j1); break;
+        case LCSS: k_glb_tq<LCSS><<<c->sm_count * 8, 256, sm1, c->stream>>>(g, j1); break;
+        default: k_glb_tq<MSM><<<c->sm_count * 8, 256, sm1, c->stream>>>(g, j1); break;
+    }
     LAUNCH_CHECK(c);
     GlbJob j2 = j1;
     double* g2t;
@@ -506,11 +516,22 @@ static int run_glb(fsmeld_ctx* c, const Geom& g, const QueryDev& qd, const Stats
     j2.in = g1; j2.in_b = g1b; j2.in_t = g1t; j2.n_in = cnt + C_G1;
     j2.out = g2; j2.out_b = nullptr; j2.out_t = g2t; j2.n_out = cnt + C_G2;
     const size_t sm2 = sizeof(double) * (((size_t)qd.m + 1) & ~(size_t)1);
-    if ((r = allow_smem(c, k_glb_qt, sm2))) return r;
+    const void* qtf = qd.metric == DTW ? (const void*)k_glb_qt<DTW>
+                    : qd.metric == ERP ? (const void*)k_glb_qt<ERP>
+                    : qd.metric == EDR ? (const void*)k_glb_qt<EDR>
+                    : qd.metric == LCSS ? (const void*)k_glb_qt<LCSS> : (const void*)k_glb_qt<MSM>;
+    if ((r = allow_smem(c, qtf, sm2))) return r;
     int per_sm = 0;
-    FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_glb_qt, 128, sm2));
+    FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qtf, 128, sm2));
+    const unsigned g2grid = (unsigned)(std::max(1, per_sm) * c->sm_count);
     prof_begin(c, ST_GLB2);
-    k_glb_qt<<<(unsigned)(std::max(1, per_sm) * c->sm_count), 128, sm2, c->stream>>>(g, j2);
+    switch (qd.metric) {
+        case DTW: k_glb_qt<DTW><<<g2grid, 128, sm2, c->stream>>>(g, j2); break;
+        case ERP: k_glb_qt<ERP><<<g2grid, 128, sm2, c->stream>>>(g, j2); break;
+        case EDR: k_glb_qt<EDR><<<g2grid, 128, sm2, c->stream>>>(g, j2); break;
+        case LCSS: k_glb_qt<LCSS><<<g2grid, 128, sm2, c->stream>>>(g, j2); break;
+        default: k_glb_qt<MSM><<<g2grid, 128, sm2, c->stream>>>(g, j2); break;
+    }
     LAUNCH_CHECK(c);
     if (out_qt) *out_qt = g2t;
     *out_list = g2;

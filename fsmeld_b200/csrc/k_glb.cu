@@ -24,11 +24,6 @@ namespace {
 __device__ __forceinline__ double edr_sub(double a, double b, double eps) {
     return (fabs(dsub(a, b)) <= eps) ? 0.0 : 1.0;
 }
-__device__ __forceinline__ bool env_match(double v, double lo, double hi, double eps) {
-    if (v < lo) return dsub(lo, v) <= eps;
-    if (v > hi) return dsub(v, hi) <= eps;
-    return true;
-}
 __device__ __forceinline__ double dminv(double a, double b) { return (a < b) ? a : b; }  // MIN macro
 __device__ __forceinline__ double dmaxv(double a, double b) { return (a > b) ? a : b; }  // MAX macro
 
@@ -47,10 +42,35 @@ __device__ __forceinline__ void warp_append(bool pred, unsigned long long* count
 
 }  // namespace
 
+// T->Q term of normalised candidate point t against the query envelope
+// [lo, hi] at the same index (src/glb.cpp:230-300), written with selects: both
+// sides are computed and one is chosen, so lanes never split on the data.
+template <int METRIC>
+__device__ __forceinline__ double tq_term(double t, double lo, double hi, double arg) {
+    if (METRIC == DTW) {
+        const double a = dsq(t, lo), b = dsq(t, hi);
+        return (t < lo) ? a : ((t > hi) ? b : 0.0);
+    } else if (METRIC == ERP) {
+        const double g2 = dsq(t, arg);
+        const double a = dminv(dsq(t, hi), g2), b = dminv(dsq(t, lo), g2);
+        return (t > hi) ? a : ((t < lo) ? b : 0.0);
+    } else if (METRIC == EDR) {
+        const double a = edr_sub(t, hi, arg), b = edr_sub(t, lo, arg);
+        return (t > hi) ? a : ((t < lo) ? b : 0.0);
+    } else if (METRIC == LCSS) {  // match indicator
+        const bool a = dsub(lo, t) <= arg, b = dsub(t, hi) <= arg;
+        return ((t < lo) ? a : ((t > hi) ? b : true)) ? 1.0 : 0.0;
+    } else {  // MSM
+        const double a = dminv(fabs(dsub(t, hi)), arg), b = dminv(fabs(dsub(t, lo)), arg);
+        return (t > hi) ? a : ((t < lo) ? b : 0.0);
+    }
+}
+
+template <int METRIC>
 __global__ void __launch_bounds__(256) k_glb_tq(Geom g, GlbJob job) {
     extern __shared__ double gq_smem[];
     const QueryDev& q = job.q;
-    const int m = q.m, metric = q.metric;
+    const int m = q.m;
     double* Q = gq_smem;
     double* LQ = Q + m;
     double* UQ = LQ + m;
@@ -58,6 +78,7 @@ __global__ void __launch_bounds__(256) k_glb_tq(Geom g, GlbJob job) {
     __syncthreads();
     const double bsf = q.cutoff;
     const double sq = dmul(bsf, bsf);  // glb_exceeds_squared_bsf, src/glb.cpp:28-31
+    const double lim = (METRIC == DTW || METRIC == ERP) ? sq : bsf;
     const double arg = q.arg;
     const unsigned long long n_in = *job.n_in;
     const unsigned long long n_lim = n_in < (unsigned long long)job.in_cap ? n_in : job.in_cap;
@@ -81,61 +102,55 @@ __global__ void __launch_bounds__(256) k_glb_tq(Geom g, GlbJob job) {
         if (active) {
 #define TN(k) ddiv(dsub(tp[(k)], mu), sg)
             const double T0 = TN(0), TL = TN(m - 1);
-            switch (metric) {
-                case DTW:
-                    boundary = dadd(dsq(T0, Q[0]), dsq(TL, Q[m - 1]));
-                    for (int k = 1; k < m - 1; ++k) {
-                        const double t = TN(k);
-                        if (t < LQ[k]) tq = dadd(tq, dsq(t, LQ[k]));
-                        else if (t > UQ[k]) tq = dadd(tq, dsq(t, UQ[k]));
-                        if (dadd(boundary, tq) > sq) { alive = false; break; }
-                    }
-                    break;
-                case ERP:
-                    boundary = dmin3(dsq(Q[m - 1], TL), dsq(Q[m - 1], arg), dsq(TL, arg));
-                    for (int k = 1; k < m - 1; ++k) {
-                        const double t = TN(k);
-                        if (t > UQ[k]) tq = dadd(tq, dminv(dsq(t, UQ[k]), dsq(t, arg)));
-                        else if (t < LQ[k]) tq = dadd(tq, dminv(dsq(t, LQ[k]), dsq(t, arg)));
-                        if (dadd(boundary, tq) > sq) { alive = false; break; }
-                    }
-                    break;
-                case EDR:
-                    boundary = dminv(edr_sub(Q[m - 1], TL, arg), 1.0);
-                    for (int k = 1; k < m - 1; ++k) {
-                        const double t = TN(k);
-                        if (t > UQ[k]) tq = dadd(tq, edr_sub(t, UQ[k], arg));
-                        else if (t < LQ[k]) tq = dadd(tq, edr_sub(t, LQ[k], arg));
-                        if (dadd(boundary, tq) > bsf) { alive = false; break; }
-                    }
-                    break;
-                case LCSS: {
-                    const double min_len = (double)m;
-                    for (int k = 0; k < m; ++k) {
-                        const double t = (k == 0) ? T0 : ((k == m - 1) ? TL : TN(k));
-                        if (env_match(t, LQ[k], UQ[k], arg)) tq = dadd(tq, 1.0);
-                    }
-                    if (dmax0(dsub(1.0, ddiv(tq, min_len))) > bsf) alive = false;
-                    break;
+            if (METRIC == DTW) {
+                boundary = dadd(dsq(T0, Q[0]), dsq(TL, Q[m - 1]));
+            } else if (METRIC == ERP) {
+                boundary = dmin3(dsq(Q[m - 1], TL), dsq(Q[m - 1], arg), dsq(TL, arg));
+            } else if (METRIC == EDR) {
+                boundary = dminv(edr_sub(Q[m - 1], TL, arg), 1.0);
+            } else if (METRIC == MSM) {
+                const double T2 = TN(m - 2);
+                const double q0 = Q[0], ql = Q[m - 1], ql2 = Q[m - 2];
+                if ((T2 >= TL && TL >= ql) || (T2 <= TL && TL <= ql) || (ql2 <= ql && ql <= TL) ||
+                    (ql2 >= ql && ql >= TL)) {
+                    boundary = dadd(fabs(dsub(q0, T0)), dminv(fabs(dsub(ql, TL)), arg));
+                } else {
+                    boundary = dadd(fabs(dsub(q0, T0)),
+                                    dmin3(fabs(dsub(ql, TL)), dadd(arg, fabs(dsub(TL, T2))),
+                                          dadd(arg, fabs(dsub(ql, ql2)))));
                 }
-                default: {  // MSM
-                    const double T2 = TN(m - 2);
-                    const double q0 = Q[0], ql = Q[m - 1], ql2 = Q[m - 2];
-                    if ((T2 >= TL && TL >= ql) || (T2 <= TL && TL <= ql) || (ql2 <= ql && ql <= TL) ||
-                        (ql2 >= ql && ql >= TL)) {
-                        boundary = dadd(fabs(dsub(q0, T0)), dminv(fabs(dsub(ql, TL)), arg));
-                    } else {
-                        boundary = dadd(fabs(dsub(q0, T0)),
-                                        dmin3(fabs(dsub(ql, TL)), dadd(arg, fabs(dsub(TL, T2))),
-                                              dadd(arg, fabs(dsub(ql, ql2)))));
-                    }
-                    for (int k = 1; k < m - 1; ++k) {
-                        const double t = TN(k);
-                        if (t > UQ[k]) tq = dadd(tq, dminv(fabs(dsub(t, UQ[k])), arg));
-                        else if (t < LQ[k]) tq = dadd(tq, dminv(fabs(dsub(t, LQ[k])), arg));
-                        if (dadd(boundary, tq) > bsf) { alive = false; break; }
-                    }
-                    break;
+            }
+            if (METRIC == LCSS) {
+                // every point, no abandon (src/glb.cpp:238-252)
+                const double min_len = (double)m;
+                int k = 0;
+                for (; k + 4 <= m; k += 4) {
+                    double t4[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) t4[u] = tq_term<LCSS>(TN(k + u), LQ[k + u], UQ[k + u], arg);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) tq = dadd(tq, t4[u]);
+                }
+                for (; k < m; ++k) tq = dadd(tq, tq_term<LCSS>(TN(k), LQ[k], UQ[k], arg));
+                if (dmax0(dsub(1.0, ddiv(tq, min_len))) > bsf) alive = false;
+            } else {
+                // points 1..m-2 four at a time: the four normalisations are
+                // independent, the sum takes them in the reference's order, and
+                // the abandon test runs once per group -- the sum never
+                // decreases, so a sum past the limit anywhere in the group is
+                // past it at the group's end (the same decision)
+                int k = 1;
+                for (; k + 4 <= m - 1; k += 4) {
+                    double t4[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) t4[u] = tq_term<METRIC>(TN(k + u), LQ[k + u], UQ[k + u], arg);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) tq = dadd(tq, t4[u]);
+                    if (dadd(boundary, tq) > lim) { alive = false; break; }
+                }
+                if (alive) {
+                    for (; k < m - 1; ++k) tq = dadd(tq, tq_term<METRIC>(TN(k), LQ[k], UQ[k], arg));
+                    if (dadd(boundary, tq) > lim) alive = false;
                 }
             }
 #undef TN
@@ -174,10 +189,11 @@ __global__ void __launch_bounds__(256) k_fwd_env(const double* __restrict__ t, l
 }
 
 // one lane per T->Q survivor: Q->T terms added in the reference's order
+template <int METRIC>
 __global__ void __launch_bounds__(128) k_glb_qt(Geom g, GlbJob job) {
     extern __shared__ double gqt_smem[];
     const QueryDev& q = job.q;
-    const int m = q.m, metric = q.metric, w = q.w;
+    const int m = q.m, w = q.w;
     double* Q = gqt_smem;
     for (int i = threadIdx.x; i < m; i += blockDim.x) Q[i] = q.qn[i];
     __syncthreads();
@@ -199,14 +215,18 @@ __global__ void __launch_bounds__(128) k_glb_qt(Geom g, GlbJob job) {
             glb = kGlbMax;  // abandoned in T->Q but MAX_VAL <= cutoff
         } else {
             const double mu = job.MU[s * g.kml + j], sg = job.SIG[s * g.kml + j];
-            const int k0 = (metric == LCSS) ? 0 : 1, k1 = (metric == LCSS) ? m - 1 : m - 2;
-            for (int k = k0; k <= k1; ++k)
-                qt = dadd(qt, qt_term(metric, Q[k], k, m, w, job.lraw + gi, job.uraw + gi, mu, sg, arg));
-            if (metric == LCSS) {
+            const double* lf = job.lraw + gi;
+            const double* uf = job.uraw + gi;
+            const int k0 = (METRIC == LCSS) ? 0 : 1, k1 = (METRIC == LCSS) ? m - 1 : m - 2;
+            // the terms are independent (unrolled so their loads and divisions
+            // overlap); only the sum is sequential, in the reference's order
+#pragma unroll 4
+            for (int k = k0; k <= k1; ++k) qt = dadd(qt, qt_term(METRIC, Q[k], k, m, w, lf, uf, mu, sg, arg));
+            if (METRIC == LCSS) {
                 glb = dmax0(dsub(1.0, ddiv(dminv(tq, qt), (double)m)));
             } else {
                 const double tot = dadd(boundary, qt);
-                if (metric == DTW || metric == ERP)
+                if (METRIC == DTW || METRIC == ERP)
                     glb = (tot > sq) ? kGlbMax : dsqrt(dmax0(dadd(boundary, dmaxv(tq, qt))));
                 else
                     glb = (tot > bsf) ? kGlbMax : dadd(boundary, dmaxv(tq, qt));
@@ -222,5 +242,14 @@ __global__ void __launch_bounds__(128) k_glb_qt(Geom g, GlbJob job) {
         }
     }
 }
+
+#define FSM_GLB_INST(M)                                       \
+    template __global__ void k_glb_tq<M>(Geom, GlbJob);       \
+    template __global__ void k_glb_qt<M>(Geom, GlbJob);
+FSM_GLB_INST(DTW)
+FSM_GLB_INST(ERP)
+FSM_GLB_INST(EDR)
+FSM_GLB_INST(LCSS)
+FSM_GLB_INST(MSM)
 
 }  // namespace fsm

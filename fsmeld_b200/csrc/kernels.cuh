@@ -84,7 +84,9 @@ __global__ void k_threshold(Geom g, const ThrJob* __restrict__ jobs, unsigned ch
                             long long slot_stride);
 template <int T>
 __global__ void k_lbip(Geom g, LbJob job, const double2* __restrict__ W, int P, int logP);
+template <int METRIC>
 __global__ void k_glb_tq(Geom g, GlbJob job);
+template <int METRIC>
 __global__ void k_glb_qt(Geom g, GlbJob job);
 __global__ void k_fwd_env(const double* __restrict__ t, long long n, int w, double* __restrict__ lo,
                           double* __restrict__ up);
