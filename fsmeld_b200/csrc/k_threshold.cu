@@ -123,7 +123,6 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
     __shared__ typename AReduce::TempStorage red_tmp;
     __shared__ int s_nr, s_nfin, s_best, s_nops;
     __shared__ int s_cnt[2];
-    __shared__ double s_init[4];
 
     const ThrJob& job = jobs[blockIdx.y];
     const QueryDev& q = job.q;
@@ -399,29 +398,32 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
             }
         }
         __syncthreads();
-        if (t == 0) {
-            double mp0 = 0.0, mp1 = 0.0, mp2 = 0.0, C = 0.0;
-#define FSM_ADD_PW(j) { const double* o_ = st + 4 * (j); mp0 = dadd(mp0, o_[0]); mp1 = dadd(mp1, o_[1]); mp2 = dadd(mp2, o_[2]); }
-            if (kind == 0) {
-                if (!upper) { for (int j = 0; j <= pl.idx1; ++j) FSM_ADD_PW(j) }
-                else { for (int j = pl.idx1; j < m; ++j) FSM_ADD_PW(j) }
-            } else if (kind == 1) {
-                if (!upper) {
-                    for (int j = pl.idx1; j > pl.idx2; --j) FSM_ADD_PW(j)
-                    for (int j = 0; j <= pl.idx2; ++j) C = dadd(C, st[4 * j + 3]);
+        // initial sums: lane j of warp 0 owns accumulator j (the power sums
+        // m_0..m_2 for j < 3, the penalty sum C for j = 3) and adds its
+        // elements in the reference's order
+        double acc = 0.0;
+        if (t < 4) {
+            const int jc = t;
+            if (jc < 3) {
+                if (kind == 0) {
+                    if (!upper) { for (int e = 0; e <= pl.idx1; ++e) acc = dadd(acc, st[4 * e + jc]); }
+                    else { for (int e = pl.idx1; e < m; ++e) acc = dadd(acc, st[4 * e + jc]); }
+                } else if (kind == 1) {
+                    if (!upper) { for (int e = pl.idx1; e > pl.idx2; --e) acc = dadd(acc, st[4 * e + jc]); }
+                    else { for (int e = pl.idx1; e < pl.idx2; ++e) acc = dadd(acc, st[4 * e + jc]); }
                 } else {
-                    for (int j = pl.idx1; j < pl.idx2; ++j) FSM_ADD_PW(j)
-                    for (int j = pl.idx2; j < m; ++j) C = dadd(C, st[4 * j + 3]);
+                    for (int e = 0; e < m; ++e)
+                        if (icode[e] == 1) acc = dadd(acc, st[4 * e + jc]);
                 }
             } else {
-                for (int e = 0; e < m; ++e) {
-                    const int cd = icode[e];
-                    if (cd == 1) FSM_ADD_PW(e)
-                    else if (cd == 2) C = dadd(C, st[4 * e + 3]);
+                if (kind == 1) {
+                    if (!upper) { for (int e = 0; e <= pl.idx2; ++e) acc = dadd(acc, st[4 * e + 3]); }
+                    else { for (int e = pl.idx2; e < m; ++e) acc = dadd(acc, st[4 * e + 3]); }
+                } else if (kind == 2) {
+                    for (int e = 0; e < m; ++e)
+                        if (icode[e] == 2) acc = dadd(acc, st[4 * e + 3]);
                 }
             }
-#undef FSM_ADD_PW
-            s_init[0] = mp0; s_init[1] = mp1; s_init[2] = mp2; s_init[3] = C;
         }
         __syncthreads();
         // op payloads into the state slots the replay overwrites
@@ -442,28 +444,29 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
             o[0] = pw0[x]; o[1] = pw0[m + x]; o[2] = pw0[2 * m + x]; o[3] = Dt[x];
         }
         __syncthreads();
-        if (t == 0) {
-            double mp0 = s_init[0], mp1 = s_init[1], mp2 = s_init[2], C = s_init[3];
-            st[0] = mp0; st[1] = mp1; st[2] = mp2; st[3] = C;
-            double* o = st + 4;
-            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        // replay: lane j applies every op to its accumulator j (op B
+        // subtracts the element's powers; op A adds them and subtracts its
+        // penalty), storing the state after each op
+        if (t < 4) {
+            const int jc = t;
+            st[jc] = acc;
+            double* o = st + 4 + jc;
+            double a = 0.0;
             int d = 0;
-            if (nops > 0) { a0 = o[0]; a1 = o[1]; a2 = o[2]; a3 = o[3]; d = opdesc[0]; }
+            if (nops > 0) { a = o[0]; d = opdesc[0]; }
             for (int k = 0; k < nops; ++k, o += 4) {
-                // next op's operands before this op's state overwrites its slot
-                double n0 = 0.0, n1 = 0.0, n2 = 0.0, n3 = 0.0;
+                // next op's operand before this op's state overwrites its slot
+                double na = 0.0;
                 int nd = 0;
-                if (k + 1 < nops) { n0 = o[4]; n1 = o[5]; n2 = o[6]; n3 = o[7]; nd = opdesc[k + 1]; }
+                if (k + 1 < nops) { na = o[4]; nd = opdesc[k + 1]; }
                 if (d >= 0) {
-                    if (d & 0x40000000) {
-                        mp0 = dsub(mp0, a0); mp1 = dsub(mp1, a1); mp2 = dsub(mp2, a2);
-                    } else {
-                        C = dsub(C, a3);
-                        mp0 = dadd(mp0, a0); mp1 = dadd(mp1, a1); mp2 = dadd(mp2, a2);
-                    }
+                    const bool op_b = (d & 0x40000000) != 0;
+                    const double sub = dsub(acc, a), add = dadd(acc, a);
+                    acc = (jc < 3) ? (op_b ? sub : add) : (op_b ? acc : sub);
                 }
-                o[0] = mp0; o[1] = mp1; o[2] = mp2; o[3] = C;
-                a0 = n0; a1 = n1; a2 = n2; a3 = n3; d = nd;
+                o[0] = acc;
+                a = na;
+                d = nd;
             }
         }
         __syncthreads();
