@@ -459,6 +459,65 @@ def impl_ours(args):
     return 0
 
 
+C4_M, C4_W, C4_KS = 512, 26, (10, 100)
+
+
+def workload_c4(args):
+    """Many DTW top-k queries (m=512, w=26, k=10 and 100) over one 2^27-point
+    walk with bursts: queries/s of the batched device-resident `cutoff`.  Each
+    measured ranking is checked against an independent path on a 2^22-point
+    prefix: the exact scan (every window through the DP) at the returned
+    threshold must give the same k smallest (distance, index) pairs."""
+    import torch
+
+    from fsmeld_b200 import api
+    from fsmeld_b200.synth import query_from, walk_with_bursts
+
+    n = args.n_points if args.n_points != N_POINTS else (1 << 27)
+    t = walk_with_bursts(n, C4_M, seed=4)
+    rng = np.random.default_rng(404)
+    qs = [query_from(t, C4_M, rng)[0] for _ in range(args.queries)]
+    eng = api.Engine(t)
+    out = {}
+    for k in C4_KS:
+        batch = [dict(query=q, m=C4_M, metric="dtw", w=C4_W, arg=0.0, k=k) for q in qs]
+        eng.batch("cutoff", batch[:2])  # warm-up (workspace, statistics)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = eng.batch("cutoff", batch)
+        wall = time.perf_counter() - t0
+        dev_ms = eng.last_call_ms
+        bad = [r["status"] for r in res if r["status"] != 0]
+        if bad:
+            raise RuntimeError(f"cutoff failed: {bad}")
+        out[k] = {"queries": len(qs), "device_ms": round(dev_ms, 2), "queries_per_s": len(qs) / (dev_ms / 1e3),
+                  "wall_queries_per_s": len(qs) / wall,
+                  "mean_threshold": float(np.mean([r["counters"]["threshold"] for r in res]))}
+    # independent check on a prefix: cutoff ranking == k smallest of the exact scan at its threshold
+    pre = t[:1 << 22]
+    checked = 0
+    with api.Engine(pre) as e2:
+        for q in qs[:4]:
+            for k in C4_KS:
+                idx, dist, _ = e2.cutoff(q, C4_M, k, "dtw", C4_W, 0.0)
+                xi, xd, _ = e2.exact(q, C4_M, float(dist[-1]), "dtw", C4_W, 0.0)
+                order = np.lexsort((xi, xd))[:k]
+                if not (np.array_equal(xi[order], idx) and np.array_equal(xd[order].view(np.int64),
+                                                                             np.asarray(dist).view(np.int64))):
+                    raise RuntimeError("cutoff ranking differs from the exact scan at its threshold")
+                checked += 1
+    eng.close()
+    peaks = load_peaks()
+    line = {"metric": "queries/s", "value": out[10]["queries_per_s"], "unit": "queries/s", "n_gpus": 1,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic (seeded random walk with bursts)",
+            "config": {"workload": f"c4: {len(qs)} DTW top-k queries, m={C4_M}, w={C4_W}, k=10 and k=100, "
+                                   f"n={n} walk + bursts on 1% of points (N(0,5))", "n": n},
+            "per_k": out, "rankings_checked_against_exact_scan": checked,
+            "hbm_peak_gbs": peaks["hbm_gbs"]}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -469,11 +528,16 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--case", choices=[m for m, _ in METRICS], help="one metric's query only (profiling runs)")
     ap.add_argument("--n-points", type=int, default=N_POINTS, help="target length (profiling runs)")
+    ap.add_argument("--workload", choices=["search5", "c4"], default="search5",
+                    help="c4: batched DTW top-k queries over a 2^27-point target (queries/s)")
+    ap.add_argument("--queries", type=int, default=32, help="c4: number of queries")
     ap.add_argument("--fixed-cutoffs", action="store_true",
                     help="use the workload's cutoff constants without recomputing them (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         return impl_reference(args)
+    if args.workload == "c4":
+        return workload_c4(args)
     return impl_ours(args)
 
 

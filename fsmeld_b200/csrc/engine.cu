@@ -481,7 +481,7 @@ enum { C_SURV, C_G1, C_G2, C_OUT, C_VALID, C_SEED, C_SEEDOUT, C_DPNEXT, C_CELLS,
 
 static int run_glb(fsmeld_ctx* c, const Geom& g, const QueryDev& qd, const Stats& st, const long long* in,
                    unsigned long long* cnt, long long cap, long long* segc, long long** out_list,
-                   double** out_qt = nullptr) {
+                   double** out_qt = nullptr, const double* cutoff_ptr = nullptr) {
     long long *g1, *g2;
     double *g1b, *g1t;
     int r;
@@ -495,6 +495,7 @@ static int run_glb(fsmeld_ctx* c, const Geom& g, const QueryDev& qd, const Stats
     j1.in = in; j1.n_in = cnt + C_SURV; j1.in_cap = cap;
     j1.out = g1; j1.out_b = g1b; j1.out_t = g1t; j1.n_out = cnt + C_G1; j1.out_cap = cap;
     j1.segc = segc;
+    j1.cutoff_ptr = cutoff_ptr;
     const size_t sm1 = sizeof(double) * 3 * qd.m;
     const void* tqf = qd.metric == DTW ? (const void*)k_glb_tq<DTW>
                     : qd.metric == ERP ? (const void*)k_glb_tq<ERP>
@@ -767,35 +768,42 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
     double* sd;
     if ((r = bufT(c, "seedi", (size_t)g.S, &si))) return r;
     if ((r = bufT(c, "seedd", (size_t)g.S, &sd))) return r;
+    // unused seed slots hold all-ones bit patterns, which sort after every distance
+    FSM_CUDA_TRY(cudaMemsetAsync(sd, 0xff, sizeof(double) * (size_t)g.S, c->stream));
     DpJob sj{};
     sj.q = qd; sj.target = c->d_target; sj.MU = st.MU; sj.SIG = st.SIG;
     sj.list = seeds; sj.n_list = cnt + C_SEED; sj.list_cap = g.S; sj.mode = 1; sj.cutoff = DBL_MAX;
     sj.out_idx = si; sj.out_dist = sd; sj.n_out = cnt + C_SEEDOUT; sj.n_cells = cnt + C_CELLS; sj.out_cap = g.S;
     if ((r = run_dp(c, g, sj, g.S))) return r;
-    FSM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
-    FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    const long long nvalid = (long long)h[C_VALID];
-    if (nvalid < qr.k) return fail(FSMELD_E_FEWER_K, "Fewer valid, non-excluded candidates than requested k.");
-    double tau = DBL_MAX;
-    const long long nseed = (long long)h[C_SEEDOUT];
-    if (nseed >= qr.k) {
-        std::vector<double> hd(nseed);
-        FSM_CUDA_TRY(cudaMemcpy(hd.data(), sd, sizeof(double) * nseed, cudaMemcpyDeviceToHost));
-        std::nth_element(hd.begin(), hd.begin() + (qr.k - 1), hd.end());
-        tau = hd[qr.k - 1];
+    // tau = k-th smallest seed distance, selected on the device: the rest of
+    // the query reads it from device memory, so the host waits only once
+    unsigned long long* sdk;
+    double* tau_dev;
+    if ((r = bufT(c, "seedsort", (size_t)g.S, &sdk))) return r;
+    if ((r = bufT(c, "tau", 1, &tau_dev))) return r;
+    {
+        size_t tmp = 0;
+        FSM_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tmp, (const unsigned long long*)sd, sdk, (int)g.S, 0,
+                                                    64, c->stream));
+        void* tp;
+        if ((r = buf(c, "seedsorttmp", tmp, &tp))) return r;
+        FSM_CUDA_TRY(cub::DeviceRadixSort::SortKeys(tp, tmp, (const unsigned long long*)sd, sdk, (int)g.S, 0, 64,
+                                                    c->stream));
+        k_tau<<<1, 32, 0, c->stream>>>(sdk, qr.k, g.S, tau_dev);
+        LAUNCH_CHECK(c);
     }
     // filter, GLB and DP at tau
     long long* f1;
     if ((r = bufT(c, "surv", (size_t)cap, &f1))) return r;
     prof_begin(c, ST_SELECT);
     k_lb_filter<<<(unsigned)std::min<long long>((g.tsn + 255) / 256, (long long)c->sm_count * 16), 256, 0, c->stream>>>(
-        g, z, st.SIG, tau, qd.metric, f1, cnt + C_SURV, cap);
+        g, z, st.SIG, tau_dev, qd.metric, f1, cnt + C_SURV, cap);
     LAUNCH_CHECK(c);
     QueryDev qt = qd;
-    qt.cutoff = tau;
+    qt.cutoff = DBL_MAX;  // the GLB kernels read tau from device memory
     long long* g2;
     double* g2t;
-    if ((r = run_glb(c, g, qt, st, f1, cnt, cap, nullptr, &g2, &g2t))) return r;
+    if ((r = run_glb(c, g, qt, st, f1, cnt, cap, nullptr, &g2, &g2t, tau_dev))) return r;
     long long* oi;
     double* od;
     if ((r = bufT(c, "outi", (size_t)cap, &oi))) return r;
@@ -803,11 +811,15 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
     DpJob dj{};
     dj.q = qt; dj.target = c->d_target; dj.MU = st.MU; dj.SIG = st.SIG;
     dj.lraw = st.Lraw; dj.uraw = st.Uraw;
-    dj.list = g2; dj.list_s = g2t; dj.n_list = cnt + C_G2; dj.list_cap = cap; dj.mode = 1; dj.cutoff = tau;
+    dj.list = g2; dj.list_s = g2t; dj.n_list = cnt + C_G2; dj.list_cap = cap; dj.mode = 1; dj.cutoff = DBL_MAX;
+    dj.cutoff_ptr = tau_dev;
     dj.out_idx = oi; dj.out_dist = od; dj.n_out = cnt + C_OUT; dj.n_cells = cnt + C_CELLS; dj.out_cap = cap;
     if ((r = run_dp(c, g, dj, (long long)c->sm_count * 16 * 128))) return r;
     FSM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
     FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const long long nvalid = (long long)h[C_VALID];
+    const long long nseed = (long long)h[C_SEEDOUT];
+    if (nvalid < qr.k) return fail(FSMELD_E_FEWER_K, "Fewer valid, non-excluded candidates than requested k.");
     const long long nout = (long long)h[C_OUT];
     if (nout < qr.k) return fail(FSMELD_E_FEWER_K, "Fewer valid, non-excluded candidates than requested k.");
     if ((r = sort_lex(c, oi, od, nout))) return r;

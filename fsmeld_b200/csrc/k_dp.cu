@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
     const unsigned long long n_all = job.list ? *job.n_list : (unsigned long long)job.n_windows;
     const unsigned long long n =
         (job.list && n_all > (unsigned long long)job.list_cap) ? job.list_cap : n_all;
-    const double cut = job.cutoff;
+    const double cut = job.cutoff_ptr ? *job.cutoff_ptr : job.cutoff;
     const double arg = q.arg;
     // abandon thresholds, once per kernel, each a little looser than the plain
     // test so that it can only abandon less: DTW/ERP sqrt(b) > s as b > s^2,

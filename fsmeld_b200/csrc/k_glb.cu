@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(256) k_glb_tq(Geom g, GlbJob job) {
     double* UQ = LQ + m;
     for (int i = threadIdx.x; i < m; i += blockDim.x) { Q[i] = q.qn[i]; LQ[i] = q.LQ[i]; UQ[i] = q.UQ[i]; }
     __syncthreads();
-    const double bsf = q.cutoff;
+    const double bsf = job.cutoff_ptr ? *job.cutoff_ptr : q.cutoff;
     const double sq = dmul(bsf, bsf);  // glb_exceeds_squared_bsf, src/glb.cpp:28-31
     const double lim = (METRIC == DTW || METRIC == ERP) ? sq : bsf;
     const double arg = q.arg;
@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(128) k_glb_qt(Geom g, GlbJob job) {
     double* Q = gqt_smem;
     for (int i = threadIdx.x; i < m; i += blockDim.x) Q[i] = q.qn[i];
     __syncthreads();
-    const double bsf = q.cutoff;
+    const double bsf = job.cutoff_ptr ? *job.cutoff_ptr : q.cutoff;
     const double sq = dmul(bsf, bsf);
     const double arg = q.arg;
     const unsigned long long n_in = *job.n_in;

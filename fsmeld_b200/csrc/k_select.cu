@@ -15,6 +15,8 @@
 //     at most the true k-th distance survives both admissible bounds;
 //  4. a lexicographic sort of the surviving (distance, index) pairs gives the
 //     ranking and the threshold.
+#include <cfloat>
+
 #include <cub/block/block_reduce.cuh>
 
 #include "common.cuh"
@@ -23,9 +25,10 @@
 namespace fsm {
 
 __global__ void __launch_bounds__(256) k_lb_filter(Geom g, const double* __restrict__ z,
-                                                   const double* __restrict__ SIG, double cutoff,
-                                                   int metric, long long* out, unsigned long long* n_out,
-                                                   long long cap) {
+                                                   const double* __restrict__ SIG,
+                                                   const double* __restrict__ cutoff_dev, int metric,
+                                                   long long* out, unsigned long long* n_out, long long cap) {
+    const double cutoff = *cutoff_dev;
     const int lane = threadIdx.x & 31;
     for (long long base = (long long)blockIdx.x * blockDim.x; base < g.tsn;
          base += (long long)gridDim.x * blockDim.x) {
@@ -83,6 +86,21 @@ __global__ void __launch_bounds__(256) k_seed(Geom g, const double* __restrict__
             if (o < (unsigned long long)cap) out[o] = r.gi;
         }
         __syncthreads();
+    }
+}
+
+// The k-th smallest seed distance, as the search bound tau: the seed
+// distances (non-negative, so their bit patterns order like the values) were
+// sorted as 64-bit keys over all n slots, the unused slots pre-filled with
+// all-ones (a NaN pattern, sorted last).  Fewer than k seeds: no bound.
+__global__ void k_tau(const unsigned long long* __restrict__ sorted, long long k, long long n, double* tau) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double v = DBL_MAX;
+        if (k >= 1 && k <= n) {
+            const double s = __longlong_as_double((long long)sorted[k - 1]);
+            if (!isnan(s)) v = s;
+        }
+        *tau = v;
     }
 }
 

@@ -46,6 +46,7 @@ struct GlbJob {
     unsigned long long* n_out;
     long long out_cap;
     long long* segc;
+    const double* cutoff_ptr;   // when set: the cutoff in device memory (read at kernel start)
 };
 
 struct DpJob {
@@ -71,6 +72,7 @@ struct DpJob {
     double* gwork;              // global band scratch when shared memory is too small
     int force_exact;            // every candidate in the DP's exact boundary mode
     unsigned long long* n_cells;  // band cells computed (optional)
+    const double* cutoff_ptr;   // when set: the cutoff in device memory (read at kernel start)
 };
 
 __global__ void k_mvmean(const double* __restrict__ target, Geom g, double* __restrict__ mu,
@@ -93,8 +95,9 @@ __global__ void k_fwd_env(const double* __restrict__ t, long long n, int w, doub
 template <int METRIC>
 __global__ void k_dp(Geom g, DpJob job);
 __global__ void k_lb_filter(Geom g, const double* __restrict__ z, const double* __restrict__ SIG,
-                            double cutoff, int metric, long long* out, unsigned long long* n_out,
-                            long long cap);
+                            const double* __restrict__ cutoff, int metric, long long* out,
+                            unsigned long long* n_out, long long cap);
+__global__ void k_tau(const unsigned long long* __restrict__ sorted, long long k, long long n, double* tau);
 __global__ void k_seed(Geom g, const double* __restrict__ z, const double* __restrict__ SIG, int per_seg,
                        long long* out, unsigned long long* n_out, long long cap);
 

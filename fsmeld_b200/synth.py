@@ -90,3 +90,18 @@ def config2(n: int = 1 << 24, m: int = 256, seed: int = 2):
         q, s = query_from(t, m, rng)
         queries[metric] = (q, s)
     return t, queries, {"m": m, "w": 13, "args": dict(CONFIG_METRIC_ARGS)}
+
+
+def walk_with_bursts(n: int, m: int, seed, burst_fraction: float = 0.01, burst_sigma: float = 5.0) -> np.ndarray:
+    """Random walk with bursts: spans of length U(m, 8m) covering `burst_fraction`
+    of the points carry extra N(0, burst_sigma) noise (the top-k workload with
+    k=10/100 over a 2^27-point target)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.standard_normal(n))
+    covered = 0
+    while covered < burst_fraction * n:
+        ln = int(rng.integers(m, 8 * m + 1))
+        s = int(rng.integers(0, max(1, n - ln)))
+        t[s:s + ln] += rng.normal(0.0, burst_sigma, size=min(ln, n - s))
+        covered += ln
+    return t
