@@ -32,6 +32,20 @@
 
 namespace fsm {
 
+// The dynamic shared-memory limit of a kernel is a process-wide attribute
+// (per device), so every context raises it through this one record and no
+// context ever lowers it under another's launches.
+cudaError_t raise_smem_limit(const void* kernel, int device, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> set;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& cur = set[{device, kernel}];
+    if (cur >= bytes) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
+
 thread_local std::string g_last_error;
 
 int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
@@ -191,7 +205,6 @@ struct fsmeld_ctx {
     struct Buf { void* p = nullptr; size_t bytes = 0; };
     std::map<std::string, Buf> bufs;
     std::map<int, double2*> twiddles;
-    std::map<const void*, int> smem_set;
     // opt-in per-stage device timing (CUDA events around each launch)
     bool prof = false;
     struct ProfRec { int stage; cudaEvent_t a, b; };
@@ -236,11 +249,8 @@ static int bufT(fsmeld_ctx* c, const std::string& name, size_t count, T** out) {
 template <typename K>
 static int allow_smem(fsmeld_ctx* c, K kernel, size_t bytes) {
     if (bytes > (size_t)c->smem_optin) return fail(FSMELD_E_UNSUPPORTED, "shared memory request too large");
-    int& cur = c->smem_set[(const void*)kernel];
-    if ((size_t)cur < bytes) {
-        FSM_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-        cur = (int)bytes;
-    }
+    const cudaError_t e = fsm::raise_smem_limit((const void*)kernel, c->device, bytes);
+    if (e != cudaSuccess) return fsm::cuda_fail(e, "cudaFuncSetAttribute", __FILE__, __LINE__);
     return FSMELD_OK;
 }
 

@@ -101,6 +101,10 @@ __global__ void k_tau(const unsigned long long* __restrict__ sorted, long long k
 __global__ void k_seed(Geom g, const double* __restrict__ z, const double* __restrict__ SIG, int per_seg,
                        long long* out, unsigned long long* n_out, long long cap);
 
+// raise a kernel's dynamic shared-memory limit on a device to at least `bytes`
+// (process-wide, never lowered; the device must be current)
+cudaError_t raise_smem_limit(const void* kernel, int device, size_t bytes);
+
 size_t mvmean_smem_bytes();
 size_t envelope_work_bytes(int m_k);
 size_t threshold_work_bytes(int cap_items, size_t sort_tmp, int m);

@@ -195,7 +195,7 @@ extern "C" int fsmeld_exact_noalloc(int device, const double* device_target, int
         return cuda_fail(e, "cudaMemsetAsync", __FILE__, __LINE__);
 
     const size_t sm_stats = mvmean_smem_bytes();
-    if ((e = cudaFuncSetAttribute(k_mvmean, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_stats)) != cudaSuccess)
+    if ((e = raise_smem_limit((const void*)k_mvmean, device, sm_stats)) != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute", __FILE__, __LINE__);
     k_mvmean<<<(unsigned)((g.S + 31) / 32), 32, sm_stats, st>>>(device_target, g, MU, SIG);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "k_mvmean", __FILE__, __LINE__);
@@ -215,7 +215,7 @@ extern "C" int fsmeld_exact_noalloc(int device, const double* device_target, int
         case LCSS: kf = (const void*)k_dp<LCSS>; break;
         default: kf = (const void*)k_dp<MSM>; break;
     }
-    if ((e = cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+    if ((e = raise_smem_limit(kf, device, smem)) != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute", __FILE__, __LINE__);
     int per_sm = 0;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf, warps * 32, smem)) != cudaSuccess)

@@ -1,0 +1,121 @@
+"""The serving loop's host logic (fsmeld_b200.serve) with a stand-in engine:
+requests are grouped by target and mode in arrival order, every answer
+reaches its own future, admission by HBM footprint rejects what does not fit
+and serves the rest, and a result larger than the batch buffer is fetched
+alone."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from fsmeld_b200.serve import E_NOMEM, Server, ServerError, footprint
+
+
+class FakeEngine:
+    """Answers from the query values: idx = [sum-derived index], one batch log."""
+
+    def __init__(self, t, log, gate=None):
+        self.n = len(t)
+        self.log = log
+        self.gate = gate
+        self.limit = None
+
+    def set_workspace_limit(self, b):
+        self.limit = b
+
+    def batch(self, mode, specs):
+        if self.gate is not None:
+            self.gate.wait()
+        self.log.append((mode, len(specs)))
+        out = []
+        for s in specs:
+            key = int(round(float(np.sum(s["query"])) * 1000)) % 997
+            big = s.get("cutoff", 0.0) == 99.0
+            idx = np.array([key], dtype=np.int64)
+            out.append({"status": 0, "idx": idx, "dist": np.array([key * 0.5]), "count": 5 if big else 1,
+                        "counters": {"valid": key}})
+        return out
+
+    def search(self, q, m, cutoff, metric, w, arg, exclude=(-1, -1)):
+        return np.arange(5, dtype=np.int64), {"valid": -1}
+
+    def exact(self, q, m, cutoff, metric, w, arg, exclude=(-1, -1)):
+        return np.arange(5, dtype=np.int64), np.arange(5.0), {"valid": -1}
+
+    def close(self):
+        pass
+
+
+def _q(i, m=32):
+    return np.sin(np.arange(m) * 0.1 * (i + 1))
+
+
+def test_routing_and_grouping():
+    log = []
+    gate = threading.Event()
+    srv = Server(budget_bytes=1 << 40, max_batch=64, engine_factory=lambda t: FakeEngine(t, log, gate))
+    try:
+        srv.add_target("a", np.zeros(4096))
+        srv.add_target("b", np.zeros(8192))
+        # the first request occupies the worker; the rest queue up and come as one pass
+        first = srv.submit("a", "search", _q(100), 32, "dtw", 3, cutoff=1.0)
+        time.sleep(0.2)
+        futs = []
+        for i in range(12):
+            tgt = "a" if i % 2 else "b"
+            if i % 3 == 0:
+                futs.append((i, srv.submit(tgt, "cutoff", _q(i), 32, "dtw", 3, k=4)))
+            else:
+                futs.append((i, srv.submit(tgt, "search", _q(i), 32, "msm", 3, 0.5, cutoff=2.0)))
+        gate.set()
+        first.result(timeout=10)
+        for i, f in futs:
+            res = f.result(timeout=10)
+            key = int(round(float(np.sum(_q(i))) * 1000)) % 997
+            assert int(res[0][0]) == key
+            assert res[-1]["valid"] == key
+        # after the first call: one batch per (target, mode) group
+        groups = {("b", "cutoff"), ("a", "search"), ("a", "cutoff"), ("b", "search")}
+        assert len(log) == 1 + len(groups)
+        assert sum(nq for _, nq in log[1:]) == 12
+    finally:
+        gate.set()
+        srv.close()
+
+
+def test_admission_by_footprint():
+    log = []
+    n = 1 << 16
+    small = footprint(n, 32, "search")
+    big = footprint(n, 4096, "search")
+    assert big > small + 4 * n
+    # room for target a, its largest small request and half of another series
+    srv = Server(budget_bytes=8 * n + small + 4 * n, engine_factory=lambda t: FakeEngine(t, log))
+    try:
+        srv.add_target("a", np.zeros(n))
+        ok = srv.submit("a", "search", _q(1), 32, "dtw", 3, cutoff=1.0)
+        bad = srv.submit("a", "search", _q(2, 4096), 4096, "dtw", 3, cutoff=1.0)
+        assert ok.result(timeout=10)[0].shape == (1,)
+        with pytest.raises(ServerError) as ei:
+            bad.result(timeout=10)
+        assert ei.value.status == E_NOMEM
+        with pytest.raises(ServerError):
+            srv.add_target("b", np.zeros(n))  # its series does not fit beside a's workspace
+    finally:
+        srv.close()
+
+
+def test_large_result_fetched_alone_and_bad_requests():
+    log = []
+    srv = Server(budget_bytes=1 << 40, engine_factory=lambda t: FakeEngine(t, log))
+    try:
+        srv.add_target("a", np.zeros(4096))
+        idx, cnt = srv.submit("a", "search", _q(3), 32, "dtw", 3, cutoff=99.0).result(timeout=10)
+        assert list(idx) == [0, 1, 2, 3, 4] and cnt["valid"] == -1
+        with pytest.raises(KeyError):
+            srv.submit("nope", "search", _q(3), 32, "dtw", 3, cutoff=1.0).result(timeout=10)
+        with pytest.raises(ValueError):
+            srv.submit("a", "cutoff", _q(3), 32, "dtw", 3, cutoff=1.0)
+    finally:
+        srv.close()
