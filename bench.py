@@ -518,6 +518,110 @@ def workload_c4(args):
     return 0
 
 
+def workload_c5(args):
+    """Serving: requests with Poisson arrivals against two resident targets
+    through `fsmeld_b200.serve.Server` (continuous batching, admission by HBM
+    footprint).  m log-uniform in [64, 2048], metric uniform, w uniform in
+    [0, floor(0.1 m)], cutoff = the request's rank-ceil(1e-4 (n-m+1)) exact
+    distance (computed before the timed run).  Reports request latency
+    (submit to answer) and throughput; a sample of answers is checked against
+    the same request run alone."""
+    import math
+    import threading
+
+    import torch
+
+    from fsmeld_b200 import api
+    from fsmeld_b200.serve import Server
+    from fsmeld_b200.synth import query_from, random_walk
+
+    sizes = {"t24": 1 << 24, "t22": 1 << 22}  # 2^28 / 2^25 scaled down to bound the run
+    targets = {name: random_walk(n, seed=50 + i) for i, (name, n) in enumerate(sizes.items())}
+    rng = np.random.default_rng(505)
+    metrics = [("dtw", 0.0), ("erp", 0.0), ("edr", 0.25), ("lcss", 0.25), ("msm", 0.5)]
+    reqs = []
+    for _ in range(args.queries):
+        name = list(sizes)[int(rng.integers(0, 2))]
+        m = int(round(math.exp(rng.uniform(math.log(64), math.log(2048)))))
+        metric, arg = metrics[int(rng.integers(0, 5))]
+        w = int(rng.integers(0, int(0.1 * m) + 1))
+        q, _ = query_from(targets[name], m, rng)
+        reqs.append([name, q, m, metric, w, arg, None])
+    # cutoffs: rank ceil(1e-4 (n-m+1)) distance of each request (untimed)
+    t_pre = time.perf_counter()
+    for name, t in targets.items():
+        with api.Engine(t) as e:
+            for r in reqs:
+                if r[0] == name:
+                    k = math.ceil(1e-4 * (len(t) - r[2] + 1))
+                    _i, d, _c = e.cutoff(r[1], r[2], k, r[3], r[4], r[5])
+                    r[6] = float(d[-1])
+                    print(f"c5 cutoff {name} m={r[2]} w={r[4]} {r[3]} k={k}: {e.last_call_ms:.1f} ms",
+                          file=sys.stderr, flush=True)
+    t_pre = time.perf_counter() - t_pre
+    lat = [None] * len(reqs)
+    answers = [None] * len(reqs)
+    with Server(device=0) as srv:
+        for name, t in targets.items():
+            srv.add_target(name, t)
+        for r in reqs[:4]:  # warm-up: workspaces of the largest lengths come later and grow then
+            srv.submit(r[0], "search", r[1], r[2], r[3], r[4], r[5], cutoff=r[6]).result()
+        torch.cuda.synchronize()
+        gaps = rng.exponential(1.0 / args.rate, size=len(reqs))
+        done = threading.Event()
+        left = [len(reqs)]
+        lk = threading.Lock()
+
+        def finish(i, t0):
+            def cb(f):
+                lat[i] = time.perf_counter() - t0
+                answers[i] = f.result()[0] if f.exception() is None else None
+                with lk:
+                    left[0] -= 1
+                    if left[0] == 0:
+                        done.set()
+            return cb
+
+        t_start = time.perf_counter()
+        t_next = t_start
+        for i, r in enumerate(reqs):
+            t_next += gaps[i]
+            delay = t_next - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            t0 = time.perf_counter()
+            srv.submit(r[0], "search", r[1], r[2], r[3], r[4], r[5], cutoff=r[6]).add_done_callback(finish(i, t0))
+        if not done.wait(timeout=600):
+            raise RuntimeError("c5: requests still pending after 600 s")
+        span = time.perf_counter() - t_start
+    failed = sum(1 for a in answers if a is None)
+    # answers in the mix against the same requests alone
+    checked = 0
+    for name, t in targets.items():
+        with api.Engine(t) as e:
+            for i, r in enumerate(reqs[: min(len(reqs), 40)]):
+                if r[0] != name or answers[i] is None:
+                    continue
+                idx, _c = e.search(r[1], r[2], r[6], r[3], r[4], r[5])
+                if not np.array_equal(idx, answers[i]):
+                    raise RuntimeError(f"request {i}: answer in the mix differs from the request alone")
+                checked += 1
+    lat_ms = np.asarray([x for x in lat if x is not None]) * 1e3
+    line = {"metric": "requests/s", "value": len(reqs) / span, "unit": "requests/s", "n_gpus": 1,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic (seeded random walks)",
+            "config": {"workload": f"c5 serving: {len(reqs)} search requests, Poisson arrivals at "
+                                   f"{args.rate}/s, targets 2^24 and 2^22 points resident, m log-uniform "
+                                   "[64, 2048], metric uniform, w uniform [0, 0.1 m], cutoff = rank "
+                                   "ceil(1e-4 (n-m+1)) distance", "rate_per_s": args.rate},
+            "latency_ms": {"p50": round(float(np.percentile(lat_ms, 50)), 2),
+                           "p99": round(float(np.percentile(lat_ms, 99)), 2),
+                           "max": round(float(lat_ms.max()), 2)},
+            "failed": failed, "answers_checked_against_alone": checked,
+            "cutoff_precompute_s": round(t_pre, 1)}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -528,8 +632,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--case", choices=[m for m, _ in METRICS], help="one metric's query only (profiling runs)")
     ap.add_argument("--n-points", type=int, default=N_POINTS, help="target length (profiling runs)")
-    ap.add_argument("--workload", choices=["search5", "c4"], default="search5",
-                    help="c4: batched DTW top-k queries over a 2^27-point target (queries/s)")
+    ap.add_argument("--workload", choices=["search5", "c4", "c5"], default="search5",
+                    help="c4: batched DTW top-k queries over a 2^27-point target (queries/s); "
+                         "c5: serving loop with Poisson arrivals (latency)")
+    ap.add_argument("--rate", type=float, default=50.0, help="c5: request arrivals per second")
     ap.add_argument("--queries", type=int, default=32, help="c4: number of queries")
     ap.add_argument("--fixed-cutoffs", action="store_true",
                     help="use the workload's cutoff constants without recomputing them (profiling runs)")
@@ -538,6 +644,8 @@ def main():
         return impl_reference(args)
     if args.workload == "c4":
         return workload_c4(args)
+    if args.workload == "c5":
+        return workload_c5(args)
     return impl_ours(args)
 
 

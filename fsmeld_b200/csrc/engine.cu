@@ -369,9 +369,13 @@ static int run_stats(fsmeld_ctx* c, const Geom& g, Stats* st, const std::string&
     return FSMELD_OK;
 }
 
+// Per-block scratch areas in global memory start on 256-byte boundaries (the
+// kernels' layouts align their arrays relative to the area's start).
+static inline size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
+
 template <int T, int OPT>
 static int launch_env(fsmeld_ctx* c, const Geom& g, int w, Stats* st) {
-    const size_t work = envelope_work_bytes(g.m_k);
+    const size_t work = round256(envelope_work_bytes(g.m_k));
     double* gwork = nullptr;
     size_t smem = work;
     unsigned grid;
@@ -384,11 +388,11 @@ static int launch_env(fsmeld_ctx* c, const Geom& g, int w, Stats* st) {
     } else {
         smem = 0;
         grid = (unsigned)std::min<long long>(g.S, (long long)c->sm_count * 2);
-        if ((r = bufT(c, "envwork", (work / 8 + 1) * grid, &gwork))) return r;
+        if ((r = bufT(c, "envwork", (work / 8) * grid, &gwork))) return r;
     }
     prof_begin(c, ST_ENV);
     k_envelope<T, OPT><<<grid, T, smem, c->stream>>>(c->d_target, st->MU, st->SIG, g, w, st->Un, st->Ln,
-                                                     gwork, (long long)(work / 8 + 1));
+                                                     gwork, (long long)(work / 8));
     LAUNCH_CHECK(c);
     return FSMELD_OK;
 }
@@ -414,7 +418,7 @@ static int run_env(fsmeld_ctx* c, const Geom& g, int w, Stats* st, const std::st
 
 template <int T, int IPT>
 static int launch_thr(fsmeld_ctx* c, const Geom& g, const ThrJob* djobs, int njobs, int m) {
-    const size_t work = threshold_work_bytes(T * IPT, threshold_sort_tmp_bytes<T, IPT>(), m);
+    const size_t work = round256(threshold_work_bytes(T * IPT, threshold_sort_tmp_bytes<T, IPT>(), m));
     unsigned char* gwork = nullptr;
     size_t smem = work;
     unsigned gx;
@@ -475,6 +479,7 @@ static int run_lbip(fsmeld_ctx* c, const Geom& g, LbJob job) {
     } else {
         grid = (unsigned)std::min<long long>(g.S, (long long)c->sm_count * 2);
         unsigned char* gw;
+        smem = round256(smem);
         if ((r = bufT(c, "lbwork", smem * grid, &gw))) return r;
         job.gwork = gw;
         job.slot_stride = (long long)smem;
@@ -768,38 +773,41 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
     lj.zout = z; lj.surv = nullptr; lj.nsurv = cnt + C_SURV; lj.nvalid = cnt + C_VALID; lj.segc = nullptr;
     if ((r = run_lbip(c, g, lj))) return r;
     // seeds
+    // seeds per segment: enough for k of them (2k over all segments), at most 32
+    const int per_seg = (int)std::min<long long>(32, std::max<long long>(1, (2 * qr.k + g.S - 1) / g.S));
+    const long long nslot = g.S * per_seg;
     long long* seeds;
-    if ((r = bufT(c, "seeds", (size_t)g.S, &seeds))) return r;
+    if ((r = bufT(c, "seeds", (size_t)nslot, &seeds))) return r;
     prof_begin(c, ST_SELECT);
     k_seed<<<(unsigned)std::min<long long>(g.S, (long long)c->sm_count * 8), 256, 0, c->stream>>>(
-        g, z, st.SIG, 1, seeds, cnt + C_SEED, g.S);
+        g, z, st.SIG, per_seg, seeds, cnt + C_SEED, nslot);
     LAUNCH_CHECK(c);
     long long* si;
     double* sd;
-    if ((r = bufT(c, "seedi", (size_t)g.S, &si))) return r;
-    if ((r = bufT(c, "seedd", (size_t)g.S, &sd))) return r;
+    if ((r = bufT(c, "seedi", (size_t)nslot, &si))) return r;
+    if ((r = bufT(c, "seedd", (size_t)nslot, &sd))) return r;
     // unused seed slots hold all-ones bit patterns, which sort after every distance
-    FSM_CUDA_TRY(cudaMemsetAsync(sd, 0xff, sizeof(double) * (size_t)g.S, c->stream));
+    FSM_CUDA_TRY(cudaMemsetAsync(sd, 0xff, sizeof(double) * (size_t)nslot, c->stream));
     DpJob sj{};
     sj.q = qd; sj.target = c->d_target; sj.MU = st.MU; sj.SIG = st.SIG;
-    sj.list = seeds; sj.n_list = cnt + C_SEED; sj.list_cap = g.S; sj.mode = 1; sj.cutoff = DBL_MAX;
-    sj.out_idx = si; sj.out_dist = sd; sj.n_out = cnt + C_SEEDOUT; sj.n_cells = cnt + C_CELLS; sj.out_cap = g.S;
-    if ((r = run_dp(c, g, sj, g.S))) return r;
+    sj.list = seeds; sj.n_list = cnt + C_SEED; sj.list_cap = nslot; sj.mode = 1; sj.cutoff = DBL_MAX;
+    sj.out_idx = si; sj.out_dist = sd; sj.n_out = cnt + C_SEEDOUT; sj.n_cells = cnt + C_CELLS; sj.out_cap = nslot;
+    if ((r = run_dp(c, g, sj, nslot))) return r;
     // tau = k-th smallest seed distance, selected on the device: the rest of
     // the query reads it from device memory, so the host waits only once
     unsigned long long* sdk;
     double* tau_dev;
-    if ((r = bufT(c, "seedsort", (size_t)g.S, &sdk))) return r;
+    if ((r = bufT(c, "seedsort", (size_t)nslot, &sdk))) return r;
     if ((r = bufT(c, "tau", 1, &tau_dev))) return r;
     {
         size_t tmp = 0;
-        FSM_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tmp, (const unsigned long long*)sd, sdk, (int)g.S, 0,
+        FSM_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, tmp, (const unsigned long long*)sd, sdk, (int)nslot, 0,
                                                     64, c->stream));
         void* tp;
         if ((r = buf(c, "seedsorttmp", tmp, &tp))) return r;
-        FSM_CUDA_TRY(cub::DeviceRadixSort::SortKeys(tp, tmp, (const unsigned long long*)sd, sdk, (int)g.S, 0, 64,
+        FSM_CUDA_TRY(cub::DeviceRadixSort::SortKeys(tp, tmp, (const unsigned long long*)sd, sdk, (int)nslot, 0, 64,
                                                     c->stream));
-        k_tau<<<1, 32, 0, c->stream>>>(sdk, qr.k, g.S, tau_dev);
+        k_tau<<<1, 32, 0, c->stream>>>(sdk, qr.k, nslot, tau_dev);
         LAUNCH_CHECK(c);
     }
     // filter, GLB and DP at tau

@@ -7,9 +7,11 @@
 // (distance, index) pairs among valid candidates.  The device form reaches
 // the same set without the serial scan:
 //  1. LB_IP per window (k_lbip with z output);
-//  2. seeds: the window with the smallest LB of each segment (k_seg_argmin);
-//     the k-th smallest exact distance among the best seeds is an upper
-//     bound tau on the k-th smallest distance overall;
+//  2. seeds: the windows with the smallest LB of each segment (k_seed,
+//     ceil(2k/S) per segment, at most 32, so that there are at least k seeds
+//     unless k > 32 S); the k-th smallest exact distance among the seeds is
+//     an upper bound tau on the k-th smallest distance overall (with fewer
+//     than k seeds there is no bound and every candidate is evaluated);
 //  3. every valid window whose LB does not exceed tau (k_lb_filter) goes
 //     through GLB at tau and then the exact DP; any window whose distance is
 //     at most the true k-th distance survives both admissible bounds;
@@ -64,28 +66,40 @@ struct MinZOp {
     }
 };
 
-// one block per segment: the valid window with the smallest LB (ties: lowest index)
+// one block per segment: its per_seg valid windows with the smallest LB
+// (ties: lowest index), by repeated block-wide argmin strictly after the
+// previous pick in (LB, index) order
 __global__ void __launch_bounds__(256) k_seed(Geom g, const double* __restrict__ z,
                                               const double* __restrict__ SIG, int per_seg,
                                               long long* out, unsigned long long* n_out, long long cap) {
     using Red = cub::BlockReduce<MinZ, 256>;
     __shared__ typename Red::TempStorage tmp;
-    (void)per_seg;
+    __shared__ MinZ s_last;
     for (long long s = blockIdx.x; s < g.S; s += gridDim.x) {
-        MinZ best{INFINITY, -1};
-        for (int j = g.lo(s) + threadIdx.x; j < g.kml; j += blockDim.x) {
-            const long long gi = g.gidx(s, j);
-            if (window_invalid(SIG[s * g.kml + j], g, gi)) continue;
-            double zz = z[s * g.kml + j];
-            if (isnan(zz)) zz = INFINITY;
-            best = MinZOp()(best, MinZ{zz, gi});
+        MinZ last{-INFINITY, -1};
+        for (int p = 0; p < per_seg; ++p) {
+            MinZ best{INFINITY, -1};
+            for (int j = g.lo(s) + threadIdx.x; j < g.kml; j += blockDim.x) {
+                const long long gi = g.gidx(s, j);
+                if (window_invalid(SIG[s * g.kml + j], g, gi)) continue;
+                double zz = z[s * g.kml + j];
+                if (isnan(zz)) zz = INFINITY;
+                if (zz < last.z || (zz == last.z && gi <= last.gi)) continue;  // picked already
+                best = MinZOp()(best, MinZ{zz, gi});
+            }
+            const MinZ r = Red(tmp).Reduce(best, MinZOp());
+            if (threadIdx.x == 0) {
+                s_last = r;
+                if (r.gi >= 0) {
+                    const unsigned long long o = atomicAdd(n_out, 1ull);
+                    if (o < (unsigned long long)cap) out[o] = r.gi;
+                }
+            }
+            __syncthreads();
+            last = s_last;
+            __syncthreads();
+            if (last.gi < 0) break;
         }
-        const MinZ r = Red(tmp).Reduce(best, MinZOp());
-        if (threadIdx.x == 0 && r.gi >= 0) {
-            const unsigned long long o = atomicAdd(n_out, 1ull);
-            if (o < (unsigned long long)cap) out[o] = r.gi;
-        }
-        __syncthreads();
     }
 }
 

@@ -293,3 +293,34 @@ def test_dp_forced_exact_mode(api, oracle, structured, monkeypatch):
             gidx, gdist, _ = e.cutoff(q, m, 9, metric, w, arg)
         oidx, odist, _ = oracle.cutoff(t, q, m, 9, metric, w, arg)
         assert list(gidx) == list(oidx) and bits_equal(gdist, odist), metric
+
+
+@pytest.mark.parametrize("m,w", [(1025, 10), (777, 0)])
+def test_long_odd_queries_vs_oracle(api, oracle, m, w):
+    # long queries (m_k = 16384 / 8192): thresholds, envelopes and LB_IP run
+    # from per-block scratch in global memory; odd m gives odd-sized layouts
+    t = walk_with_structure(1 << 17, m, seed=1000 + m, motifs=8, nan_fraction=1e-3, flat_runs=2, nan_spans=2)
+    q, _ = query_from(t, m, np.random.default_rng(m))
+    with api.Engine(t) as e:
+        for metric, arg in [("dtw", 0.0), ("erp", 0.4), ("lcss", 0.25)]:
+            gidx, gdist, _ = e.cutoff(q, m, 5, metric, w, arg)
+            oidx, odist, _ = oracle.cutoff(t, q, m, 5, metric, w, arg)
+            assert list(gidx) == list(oidx) and bits_equal(gdist, odist), metric
+            cut = float(odist[-1])
+            sidx, sc = e.search(q, m, cut, metric, w, arg)
+            xidx, xc = oracle.search(t, q, m, cut, metric, w, arg)
+            assert list(sidx) == list(xidx), metric
+            assert sc["valid"] == xc["valid"]
+
+
+def test_cutoff_k_larger_than_segments(api, oracle):
+    # k far above the number of macro segments: several seeds per segment
+    m, w = 64, 4
+    t = walk_with_structure(4000, m, seed=4242, motifs=3, nan_fraction=0.0, flat_runs=1)
+    q, _ = query_from(t, m, np.random.default_rng(4243))
+    with api.Engine(t) as e:
+        for metric, arg in [("dtw", 0.0), ("edr", 0.25), ("msm", 0.5)]:
+            for k in (40, 200):
+                gidx, gdist, _ = e.cutoff(q, m, k, metric, w, arg)
+                oidx, odist, _ = oracle.cutoff(t, q, m, k, metric, w, arg)
+                assert list(gidx) == list(oidx) and bits_equal(gdist, odist), (metric, k)
