@@ -127,6 +127,43 @@ __device__ __forceinline__ double qt_term_env(int metric, double x, double a, do
     }
 }
 
+// The same term for the DP's cascading abandon test, without divisions: the
+// window bounds are scaled by inv = fl(1/sigma) (relative error ~2^-52) and
+// the envelope is then narrowed by a relative 2^-49 (lo raised, up lowered),
+// so it lies inside the exact envelope.  Every term is then at least the
+// exact term (DTW/ERP/EDR/MSM: distances to a narrower envelope) and LCSS's
+// match indicator at most the exact one; the abandon bound built from these
+// terms can only be looser than the exact one, never tighter.
+__device__ __forceinline__ double qt_term_bound(int metric, double x, double a, double b, double mu, double inv,
+                                                double arg) {
+    double lo = dmul(dsub(a, mu), inv);
+    double up = dmul(dsub(b, mu), inv);
+    lo = dadd(lo, dadd(dmul(fabs(lo), 0x1p-49), 0x1p-1000));
+    up = dsub(up, dadd(dmul(fabs(up), 0x1p-49), 0x1p-1000));
+    switch (metric) {
+        case DTW:
+            if (x < lo) return dsq(x, lo);
+            if (x > up) return dsq(x, up);
+            return 0.0;
+        case ERP:
+            if (x > up) { const double p = dsq(x, up), r = dsq(x, arg); return (p < r) ? p : r; }
+            if (x < lo) { const double p = dsq(x, lo), r = dsq(x, arg); return (p < r) ? p : r; }
+            return 0.0;
+        case EDR:
+            if (x > up) return (fabs(dsub(x, up)) <= arg) ? 0.0 : 1.0;
+            if (x < lo) return (fabs(dsub(x, lo)) <= arg) ? 0.0 : 1.0;
+            return 0.0;
+        case LCSS:
+            if (x < lo) return (dsub(lo, x) <= arg) ? 1.0 : 0.0;
+            if (x > up) return (dsub(x, up) <= arg) ? 1.0 : 0.0;
+            return 1.0;
+        default:
+            if (x > up) { const double p = fabs(dsub(x, up)); return (p < arg) ? p : arg; }
+            if (x < lo) { const double p = fabs(dsub(x, lo)); return (p < arg) ? p : arg; }
+            return 0.0;
+    }
+}
+
 __device__ __forceinline__ double qt_term(int metric, double x, int k, int m, int w, const double* lf,
                                           const double* uf, double mu, double sg, double arg) {
     const int p0 = qt_p0(k, w), p1 = qt_p1(k, m, w);

@@ -44,8 +44,10 @@
 // plus, for every later row, the GLB's per-point Q->T term (the cheapest way
 // to align that query point with the candidate's envelope).  The GLB stage
 // hands over each survivor's Q->T sum; the DP subtracts the terms of the rows
-// it has done.  A candidate whose bound already exceeds the cutoff (with a
-// 1e-9 relative slack for round-off) cannot be kept and stops.  For LCSS the
+// it has done (terms computed without divisions on a slightly narrowed
+// envelope, which only loosens the bound).  A candidate whose bound already
+// exceeds the cutoff (with a 1e-9 relative slack for round-off) cannot be
+// kept and stops.  For LCSS the
 // final match count is at most the row maximum plus the matches the
 // remaining rows can still reach.  Out-of-band cells can only lower a row
 // minimum (raise an LCSS row maximum), which keeps the bound valid.  Results
@@ -221,7 +223,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
     const double* tp = job.target;
     const double* lr = job.lraw;
     const double* ur = job.uraw;
-    double mu = 0.0, sg = 1.0;
+    double mu = 0.0, sg = 1.0, inv = 1.0;
     int row = 0, ny = 0;
     double Ssum = 0.0, Pre = 0.0;  // GLB Q->T sum of the candidate, and its prefix over rows done
     bool has_s = false;
@@ -322,6 +324,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
                     sg = job.SIG[s * g.kml + j];
                     if (!window_invalid(sg, g, gi)) {
                         tp = job.target + gi;
+                        inv = ddiv(1.0, sg);
                         if (job.lraw) { lr = job.lraw + gi; ur = job.uraw + gi; }
                         ++valid_count;
                         has_s = job.list_s && job.lraw && job.list_s[c] >= 0.0;
@@ -430,7 +433,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
         const bool use_term = has_s && (METRIC == LCSS || (k >= 1 && k <= m - 2));
         const double ta = fmin(na0, na1), tb = fmax(nb0, nb1);
         if (i < last) prefetch(i + 1);  // next row's loads overlap this row's cells
-        const double term = use_term ? qt_term_env(METRIC, rc.xi, ta, tb, mu, sg, arg) : 0.0;
+        const double term = use_term ? qt_term_bound(METRIC, rc.xi, ta, tb, mu, inv, arg) : 0.0;
         double ext;
         if (!exact) {
             ext = dp_row<METRIC, false>(A, R, RM, W2, s0, rc, arg, 0, 0, -1);
