@@ -80,6 +80,7 @@ def lib():
             "fsmeld_last_error": (C.c_char_p, [ctxp]),
             "fsmeld_strerror": (C.c_char_p, [C.c_int]),
             "fsmeld_set_workspace_limit": (C.c_int, [ctxp, C.c_int64]),
+            "fsmeld_set_concurrency": (C.c_int, [ctxp, C.c_int]),
             "fsmeld_kernel_launches": (C.c_int64, [ctxp]),
             "fsmeld_set_profiling": (C.c_int, [ctxp, C.c_int]),
             "fsmeld_stage_times": (C.c_int, [ctxp, dp, ip, C.c_int]),
@@ -200,6 +201,10 @@ class Engine:
 
     def set_workspace_limit(self, nbytes):
         _check(lib().fsmeld_set_workspace_limit(self._ctx, int(nbytes)), self._ctx)
+
+    def set_concurrency(self, queries):
+        """Queries of one (m, w) group of a batch run concurrently on this many streams."""
+        _check(lib().fsmeld_set_concurrency(self._ctx, int(queries)), self._ctx)
 
     def search(self, query, m, cutoff, metric, w, arg=0.0, exclude=(-1, -1), seg_counts=False):
         q = np.ascontiguousarray(query[:m], dtype=np.float64)

@@ -23,6 +23,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/fsmeld_cuda.h"
@@ -197,6 +198,11 @@ struct fsmeld_ctx {
     int smem_optin = 227 * 1024;
     long long ws_limit = 0;
     long long launches = 0;
+    // queries of one batch group run concurrently on this many worker
+    // contexts (own stream and buffers, shared target, statistics, envelopes)
+    int concurrency = 4;
+    std::vector<fsmeld_ctx*> workers;
+    cudaEvent_t ev_ready = nullptr;  // shared statistics/envelopes of a group are on the device
     // FSMELD_DP_EXACT=1: run every DP candidate in the exact boundary mode
     // (same results; a diagnostic switch for the mode that in-range data never needs)
     bool dp_exact = false;
@@ -860,6 +866,36 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
 }
 
 // One call over many queries: statistics per distinct m, envelopes per distinct (m, w).
+// worker context i of c (created on first use): same device and target, its
+// own stream and grow-only buffers
+static int get_worker(fsmeld_ctx* c, int i, fsmeld_ctx** out) {
+    while ((int)c->workers.size() <= i) {
+        fsmeld_ctx* w = new fsmeld_ctx();
+        w->device = c->device;
+        w->sm_count = c->sm_count;
+        w->smem_optin = c->smem_optin;
+        w->dp_exact = c->dp_exact;
+        if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreate(&w->ev0) != cudaSuccess || cudaEventCreate(&w->ev1) != cudaSuccess) {
+            delete w;
+            return fail(FSMELD_E_CUDA, "stream/event creation failed");
+        }
+        c->workers.push_back(w);
+    }
+    fsmeld_ctx* w = c->workers[i];
+    w->d_target = c->d_target;  // borrowed: the target may have been reloaded
+    w->own_target = false;
+    w->n = c->n;
+    w->ws_limit = c->ws_limit;
+    w->prof = c->prof;
+    *out = w;
+    return FSMELD_OK;
+}
+
+// One call over many queries: statistics per distinct m, envelopes per distinct
+// (m, w); the queries of one (m, w) group then run concurrently on worker
+// streams (each query's pipeline is independent; its last step waits for its
+// own stream, so the group is done on the device when its threads return).
 int run_batch(fsmeld_ctx* c, std::vector<QueryRun>& runs, std::vector<int>* status) {
     status->assign(runs.size(), FSMELD_OK);
     std::vector<size_t> order(runs.size());
@@ -868,14 +904,17 @@ int run_batch(fsmeld_ctx* c, std::vector<QueryRun>& runs, std::vector<int>* stat
         if (runs[a].hq->m != runs[b].hq->m) return runs[a].hq->m < runs[b].hq->m;
         return runs[a].hq->w < runs[b].hq->w;
     });
+    if (!c->ev_ready) FSM_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_ready, cudaEventDisableTiming));
     int cur_m = -1, cur_w = -1;
     Stats st;
     Geom g{};
     bool have_env = false;
     int first_err = FSMELD_OK;
-    for (size_t oi = 0; oi < order.size(); ++oi) {
-        QueryRun& qr = runs[order[oi]];
-        const int m = qr.hq->m, w = qr.hq->w;
+    size_t oi = 0;
+    while (oi < order.size()) {
+        const int m = runs[order[oi]].hq->m, w = runs[order[oi]].hq->w;
+        size_t oj = oi + 1;
+        while (oj < order.size() && runs[order[oj]].hq->m == m && runs[order[oj]].hq->w == w) ++oj;
         int r = FSMELD_OK;
         if (m != cur_m) {
             have_env = false;
@@ -884,15 +923,79 @@ int run_batch(fsmeld_ctx* c, std::vector<QueryRun>& runs, std::vector<int>* stat
             if (!r) r = run_stats(c, g, &st, "");
             cur_m = r ? -1 : m;
         }
-        if (!r && qr.mode != 2 && w != cur_w) {
+        bool need_env = false;
+        for (size_t k = oi; k < oj; ++k) need_env = need_env || runs[order[k]].mode != 2;
+        if (!r && need_env && w != cur_w) {
             r = run_env(c, g, w, &st, "");
             cur_w = r ? -1 : w;
             have_env = !r;
         }
-        if (!r) r = run_query(c, qr, g, st, have_env);
-        (*status)[order[oi]] = r;
-        if (r && !first_err) first_err = r;
-        if (r == FSMELD_E_CUDA) break;
+        if (r) {
+            for (size_t k = oi; k < oj; ++k) (*status)[order[k]] = r;
+            if (!first_err) first_err = r;
+            if (r == FSMELD_E_CUDA) break;
+            oi = oj;
+            continue;
+        }
+        const int nq = (int)(oj - oi);
+        const int conc = std::min(std::max(1, c->concurrency), nq);
+        if (conc <= 1) {
+            for (size_t k = oi; k < oj; ++k) {
+                const int q = run_query(c, runs[order[k]], g, st, have_env);
+                (*status)[order[k]] = q;
+                if (q && !first_err) first_err = q;
+                if (q == FSMELD_E_CUDA) break;
+            }
+        } else {
+            FSM_CUDA_TRY(cudaEventRecord(c->ev_ready, c->stream));
+            std::vector<fsmeld_ctx*> ws(conc);
+            for (int t = 0; t < conc; ++t)
+                if ((r = get_worker(c, t, &ws[t]))) return r;
+            std::vector<std::string> errs(conc);
+            std::vector<std::thread> th;
+            for (int t = 0; t < conc; ++t) {
+                th.emplace_back([&, t] {
+                    cudaSetDevice(c->device);
+                    fsmeld_ctx* wk = ws[t];
+                    if (cudaStreamWaitEvent(wk->stream, c->ev_ready, 0) != cudaSuccess) {
+                        for (int k = t; k < nq; k += conc) (*status)[order[oi + k]] = FSMELD_E_CUDA;
+                        return;
+                    }
+                    for (int k = t; k < nq; k += conc) {
+                        const int q = run_query(wk, runs[order[oi + k]], g, st, have_env);
+                        (*status)[order[oi + k]] = q;
+                        if (q && errs[t].empty()) errs[t] = g_last_error;
+                        if (q == FSMELD_E_CUDA) break;
+                    }
+                });
+            }
+            for (auto& x : th) x.join();
+            for (int t = 0; t < conc; ++t) {
+                fsmeld_ctx* wk = ws[t];
+                // a query that failed part-way may have left kernels queued: the next
+                // group rewrites the shared statistics only after they are done
+                cudaStreamSynchronize(wk->stream);
+                prof_collect(wk);
+                for (int k = 0; k < 8; ++k) {
+                    c->stage_ms[k] += wk->stage_ms[k];
+                    c->stage_n[k] += wk->stage_n[k];
+                    wk->stage_ms[k] = 0.0;
+                    wk->stage_n[k] = 0;
+                }
+                c->launches += wk->launches;
+                wk->launches = 0;
+            }
+            for (size_t k = oi; k < oj; ++k) {
+                const int q = (*status)[order[k]];
+                if (q && !first_err) {
+                    first_err = q;
+                    for (auto& e : errs) if (!e.empty()) { g_last_error = e; break; }
+                }
+            }
+            if (first_err == FSMELD_E_CUDA) break;
+        }
+        if (first_err == FSMELD_E_CUDA) break;
+        oi = oj;
     }
     return first_err;
 }
@@ -987,6 +1090,9 @@ int fsmeld_open_file(int device, const char* path, fsmeld_ctx** out) {
 int fsmeld_close(fsmeld_ctx* c) {
     if (!c) return FSMELD_OK;
     cudaSetDevice(c->device);
+    for (auto* w : c->workers) fsmeld_close(w);  // borrowed target: not freed there
+    c->workers.clear();
+    if (c->ev_ready) cudaEventDestroy(c->ev_ready);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (auto& kv : c->bufs) if (kv.second.p) cudaFree(kv.second.p);
     for (auto& kv : c->twiddles) cudaFree(kv.second);
@@ -1001,6 +1107,12 @@ int fsmeld_close(fsmeld_ctx* c) {
 }
 
 int64_t fsmeld_target_length(const fsmeld_ctx* c) { return c ? c->n : 0; }
+
+int fsmeld_set_concurrency(fsmeld_ctx* c, int queries) {
+    if (!c || queries < 1 || queries > 16) return fail(FSMELD_E_ARG, "concurrency must be in [1, 16]");
+    c->concurrency = queries;
+    return FSMELD_OK;
+}
 
 const char* fsmeld_last_error(const fsmeld_ctx* c) {
     (void)c;

@@ -41,23 +41,28 @@ def macro_length(m: int, n: int) -> int:
     return min(mk, n)
 
 
-def footprint(n: int, m: int, mode: str) -> int:
-    """Upper estimate of the device workspace (bytes) one request needs on a
-    target of n points."""
+CONCURRENCY = 4  # queries of a batch group running at once (Engine default)
+
+
+def footprint(n: int, m: int, mode: str, concurrent: int = 1) -> int:
+    """Upper estimate of the device workspace (bytes) a request needs on a
+    target of n points, with `concurrent` queries of its batch group running
+    at once (each holds its own query buffers)."""
     mk = macro_length(m, n)
     kml = mk - m + 1
     tsn = n - m + 1
     S = -(-tsn // kml)
-    b = 16 * S * kml           # window means and sigmas
-    b += 16 * S * mk           # segment envelopes U/L_normal
-    b += 16 * n                # forward windows min/max of the raw target
-    b += 40 * tsn              # GLB stage lists (index, boundary, T->Q, survivors, Q->T)
-    b += 24 * tsn              # survivors and the (index, distance) result list
-    b += 16 * tsn              # sort buffers of the results
-    b += 48 * S                # thresholds, segment counters, seeds
+    shared = 16 * S * kml      # window means and sigmas
+    shared += 16 * S * mk      # segment envelopes U/L_normal
+    shared += 16 * n           # forward windows min/max of the raw target
+    q = 40 * tsn               # GLB stage lists (index, boundary, T->Q, survivors, Q->T)
+    q += 24 * tsn              # survivors and the (index, distance) result list
+    q += 16 * tsn              # sort buffers of the results
+    q += 48 * S                # thresholds, segment counters, seeds
     if mode == "cutoff":
-        b += 8 * S * kml + 24 * S  # LB values of every window, seed distances
-    return int(b * 1.05) + (64 << 20)  # kernel scratch (sort temporaries, work areas)
+        q += 8 * S * kml + 24 * S  # LB values of every window, seed distances
+    per_query = int(q * 1.05) + (64 << 20)  # kernel scratch (sort temporaries, work areas)
+    return int(shared * 1.05) + max(1, concurrent) * per_query
 
 
 class ServerError(RuntimeError):
@@ -195,8 +200,9 @@ class Server:
                 return
             room = self.budget - self._used(exclude=name) - 8 * tgt.n
         admitted = []
+        conc = min(CONCURRENCY, len(reqs))
         for r in reqs:
-            fp = footprint(tgt.n, r.spec["m"], mode) if r.spec["m"] <= tgt.n else 0
+            fp = footprint(tgt.n, r.spec["m"], mode, conc) if r.spec["m"] <= tgt.n else 0
             if max(tgt.workspace, fp) > room:
                 r.future.set_exception(ServerError(E_NOMEM, "request does not fit in the HBM budget"))
             else:

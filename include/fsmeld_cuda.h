@@ -109,6 +109,13 @@ int fsmeld_close(fsmeld_ctx* ctx);
 int64_t fsmeld_target_length(const fsmeld_ctx* ctx);
 const char* fsmeld_last_error(const fsmeld_ctx* ctx);
 const char* fsmeld_strerror(int status);
+/* Batched calls (fsmeld_batch): the queries of one (m, w) group run
+ * concurrently on this many worker streams of the context (1..16, default 4;
+ * 1 runs them one after another).  Each worker holds its own query buffers,
+ * so the device workspace grows with the concurrency.  No reference
+ * counterpart (the reference runs one query per process). */
+int fsmeld_set_concurrency(fsmeld_ctx* ctx, int queries);
+
 /* Cap on device workspace bytes (0 = no cap); exceeding it -> FSMELD_E_NOMEM. */
 int fsmeld_set_workspace_limit(fsmeld_ctx* ctx, int64_t bytes);
 /* Number of CUDA kernel launches issued by this context so far. */

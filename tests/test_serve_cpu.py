@@ -95,8 +95,8 @@ def test_admission_by_footprint():
     try:
         srv.add_target("a", np.zeros(n))
         ok = srv.submit("a", "search", _q(1), 32, "dtw", 3, cutoff=1.0)
+        assert ok.result(timeout=10)[0].shape == (1,)  # alone in its pass: one query's buffers
         bad = srv.submit("a", "search", _q(2, 4096), 4096, "dtw", 3, cutoff=1.0)
-        assert ok.result(timeout=10)[0].shape == (1,)
         with pytest.raises(ServerError) as ei:
             bad.result(timeout=10)
         assert ei.value.status == E_NOMEM
