@@ -572,12 +572,9 @@ static int run_dp(fsmeld_ctx* c, const Geom& g, DpJob job, long long expected) {
     job.next = next;
     job.gwork = nullptr;
     job.force_exact = c->dp_exact ? 1 : 0;
-    const void* kf = job.q.metric == DTW ? (const void*)k_dp<DTW>
-                   : job.q.metric == ERP ? (const void*)k_dp<ERP>
-                   : job.q.metric == EDR ? (const void*)k_dp<EDR>
-                   : job.q.metric == LCSS ? (const void*)k_dp<LCSS> : (const void*)k_dp<MSM>;
     unsigned grid;
-    if (smem > (size_t)c->smem_optin - 4096) {
+    const bool gw_path = smem > (size_t)c->smem_optin - 4096;
+    if (gw_path) {
         // band scratch in global memory (L2-resident per warp): 16 warps per SM
         const long long want = (expected + warps * 32 - 1) / (warps * 32);
         grid = (unsigned)std::max<long long>(1, std::min<long long>(want, (long long)c->sm_count * (16 / warps)));
@@ -586,27 +583,19 @@ static int run_dp(fsmeld_ctx* c, const Geom& g, DpJob job, long long expected) {
         job.gwork = gw;
         smem = 0;
     }
-    switch (job.q.metric) {
-        case DTW: if ((r = allow_smem(c, k_dp<DTW>, smem))) return r; break;
-        case ERP: if ((r = allow_smem(c, k_dp<ERP>, smem))) return r; break;
-        case EDR: if ((r = allow_smem(c, k_dp<EDR>, smem))) return r; break;
-        case LCSS: if ((r = allow_smem(c, k_dp<LCSS>, smem))) return r; break;
-        default: if ((r = allow_smem(c, k_dp<MSM>, smem))) return r; break;
-    }
-    if (!job.gwork) {
+    const void* kf = dp_kernel(job.q.metric, gw_path);
+    if ((r = allow_smem(c, kf, smem))) return r;
+    if (!gw_path) {
         int per_sm = 0;
         FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf, warps * 32, smem));
         const long long want = (expected + warps * 32 - 1) / (warps * 32);
         grid = (unsigned)std::max<long long>(1, std::min<long long>(want, (long long)std::max(1, per_sm) * c->sm_count));
     }
     prof_begin(c, ST_DP);
-    switch (job.q.metric) {
-        case DTW: k_dp<DTW><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
-        case ERP: k_dp<ERP><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
-        case EDR: k_dp<EDR><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
-        case LCSS: k_dp<LCSS><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
-        default: k_dp<MSM><<<grid, warps * 32, smem, c->stream>>>(g, job); break;
-    }
+    Geom ga = g;
+    void* args[] = {&ga, &job};
+    const cudaError_t le = cudaLaunchKernel(kf, dim3(grid), dim3(warps * 32), args, smem, c->stream);
+    if (le != cudaSuccess) return cuda_fail(le, "k_dp launch", __FILE__, __LINE__);
     LAUNCH_CHECK(c);
     return FSMELD_OK;
 }

@@ -171,7 +171,7 @@ __device__ __forceinline__ double dp_row(double* __restrict__ A, const double* _
 
 }  // namespace
 
-template <int METRIC>
+template <int METRIC, bool GW>
 __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
     extern __shared__ __align__(16) double dp_smem[];
     const QueryDev& q = job.q;
@@ -181,8 +181,11 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
     const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const double* __restrict__ X = q.qn;
     const size_t per_warp = dp_warp_doubles(w);
-    double* wbase = job.gwork ? job.gwork + ((size_t)blockIdx.x * warps + warp) * per_warp
-                              : dp_smem + warp * per_warp;
+    // GW: band and ring in global scratch (too wide for shared memory); the
+    // shared-memory form keeps the pointers provably shared, so every band and
+    // ring access compiles to a shared-memory access
+    double* wbase = GW ? job.gwork + ((size_t)blockIdx.x * warps + warp) * per_warp
+                       : dp_smem + warp * per_warp;
     double* const A = wbase + lane;                            // band row, A[d * 32], d in [0, W2]
     double* const R = wbase + (size_t)(W2 + 1) * 32 + lane;    // ring, R[slot * 32]
     const unsigned long long n_all = job.list ? *job.n_list : (unsigned long long)job.n_windows;
@@ -499,10 +502,23 @@ __host__ __device__ int dp_ring(int w) {
 
 __host__ __device__ size_t dp_warp_doubles(int w) { return (size_t)((2 * w + 2) + dp_ring(w)) * 32; }
 
-template __global__ void k_dp<DTW>(Geom, DpJob);
-template __global__ void k_dp<ERP>(Geom, DpJob);
-template __global__ void k_dp<EDR>(Geom, DpJob);
-template __global__ void k_dp<LCSS>(Geom, DpJob);
-template __global__ void k_dp<MSM>(Geom, DpJob);
+#define FSM_DP_INST(M)                                   \
+    template __global__ void k_dp<M, false>(Geom, DpJob); \
+    template __global__ void k_dp<M, true>(Geom, DpJob);
+FSM_DP_INST(DTW)
+FSM_DP_INST(ERP)
+FSM_DP_INST(EDR)
+FSM_DP_INST(LCSS)
+FSM_DP_INST(MSM)
+
+const void* dp_kernel(int metric, bool gw) {
+    switch (metric) {
+        case DTW: return gw ? (const void*)k_dp<DTW, true> : (const void*)k_dp<DTW, false>;
+        case ERP: return gw ? (const void*)k_dp<ERP, true> : (const void*)k_dp<ERP, false>;
+        case EDR: return gw ? (const void*)k_dp<EDR, true> : (const void*)k_dp<EDR, false>;
+        case LCSS: return gw ? (const void*)k_dp<LCSS, true> : (const void*)k_dp<LCSS, false>;
+        default: return gw ? (const void*)k_dp<MSM, true> : (const void*)k_dp<MSM, false>;
+    }
+}
 
 }  // namespace fsm

@@ -92,8 +92,10 @@ template <int METRIC>
 __global__ void k_glb_qt(Geom g, GlbJob job);
 __global__ void k_fwd_env(const double* __restrict__ t, long long n, int w, double* __restrict__ lo,
                           double* __restrict__ up);
-template <int METRIC>
+template <int METRIC, bool GW>
 __global__ void k_dp(Geom g, DpJob job);
+// the DP kernel for a metric, with its band in shared memory or in job.gwork
+const void* dp_kernel(int metric, bool gw);
 __global__ void k_lb_filter(Geom g, const double* __restrict__ z, const double* __restrict__ SIG,
                             const double* __restrict__ cutoff, int metric, long long* out,
                             unsigned long long* n_out, long long cap);

@@ -207,26 +207,17 @@ extern "C" int fsmeld_exact_noalloc(int device, const double* device_target, int
     dj.list = nullptr; dj.n_windows = g.tsn; dj.mode = 0; dj.cutoff = cutoff;
     dj.out_idx = li; dj.out_dist = ld; dj.n_out = cnt + 0; dj.out_cap = kMaxWin;
     dj.n_valid = cnt + 1; dj.next = cnt + 2; dj.gwork = nullptr;
-    const void* kf;
-    switch (metric) {
-        case DTW: kf = (const void*)k_dp<DTW>; break;
-        case ERP: kf = (const void*)k_dp<ERP>; break;
-        case EDR: kf = (const void*)k_dp<EDR>; break;
-        case LCSS: kf = (const void*)k_dp<LCSS>; break;
-        default: kf = (const void*)k_dp<MSM>; break;
-    }
+    const void* kf = dp_kernel(metric, false);
     if ((e = raise_smem_limit(kf, device, smem)) != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute", __FILE__, __LINE__);
     int per_sm = 0;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf, warps * 32, smem)) != cudaSuccess)
         return cuda_fail(e, "occupancy", __FILE__, __LINE__);
     const unsigned grid = (unsigned)std::max(1, per_sm) * (unsigned)sms;
-    switch (metric) {
-        case DTW: k_dp<DTW><<<grid, warps * 32, smem, st>>>(g, dj); break;
-        case ERP: k_dp<ERP><<<grid, warps * 32, smem, st>>>(g, dj); break;
-        case EDR: k_dp<EDR><<<grid, warps * 32, smem, st>>>(g, dj); break;
-        case LCSS: k_dp<LCSS><<<grid, warps * 32, smem, st>>>(g, dj); break;
-        default: k_dp<MSM><<<grid, warps * 32, smem, st>>>(g, dj); break;
+    {
+        void* args[] = {&g, &dj};
+        if ((e = cudaLaunchKernel(kf, dim3(grid), dim3(warps * 32), args, smem, st)) != cudaSuccess)
+            return cuda_fail(e, "k_dp", __FILE__, __LINE__);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "k_dp", __FILE__, __LINE__);
     k_noalloc_scatter<<<(unsigned)sms * 4, 256, 0, st>>>(li, ld, cnt + 0, win);
