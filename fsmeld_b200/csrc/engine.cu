@@ -386,10 +386,11 @@ static int launch_env(fsmeld_ctx* c, const Geom& g, int w, Stats* st) {
     size_t smem = work;
     unsigned grid;
     int r;
-    if (work + 8192 <= (size_t)c->smem_optin) {
-        if ((r = allow_smem(c, k_envelope<T, OPT>, smem))) return r;
+    const bool gw_path = work + 8192 > (size_t)c->smem_optin;
+    if (!gw_path) {
+        if ((r = allow_smem(c, k_envelope<T, OPT, false>, smem))) return r;
         int per_sm = 0;
-        FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_envelope<T, OPT>, T, smem));
+        FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_envelope<T, OPT, false>, T, smem));
         grid = (unsigned)std::min<long long>(g.S, (long long)std::max(1, per_sm) * c->sm_count);
     } else {
         smem = 0;
@@ -397,8 +398,12 @@ static int launch_env(fsmeld_ctx* c, const Geom& g, int w, Stats* st) {
         if ((r = bufT(c, "envwork", (work / 8) * grid, &gwork))) return r;
     }
     prof_begin(c, ST_ENV);
-    k_envelope<T, OPT><<<grid, T, smem, c->stream>>>(c->d_target, st->MU, st->SIG, g, w, st->Un, st->Ln,
-                                                     gwork, (long long)(work / 8));
+    if (gw_path)
+        k_envelope<T, OPT, true><<<grid, T, smem, c->stream>>>(c->d_target, st->MU, st->SIG, g, w, st->Un, st->Ln,
+                                                               gwork, (long long)(work / 8));
+    else
+        k_envelope<T, OPT, false><<<grid, T, smem, c->stream>>>(c->d_target, st->MU, st->SIG, g, w, st->Un, st->Ln,
+                                                                gwork, (long long)(work / 8));
     LAUNCH_CHECK(c);
     return FSMELD_OK;
 }
@@ -429,19 +434,33 @@ static int launch_thr(fsmeld_ctx* c, const Geom& g, const ThrJob* djobs, int njo
     size_t smem = work;
     unsigned gx;
     int r;
-    if (work + 16384 <= (size_t)c->smem_optin) {
-        if ((r = allow_smem(c, k_threshold<T, IPT>, smem))) return r;
+    const bool gw_path = work + 16384 > (size_t)c->smem_optin;
+    if (!gw_path) {
+        if ((r = allow_smem(c, k_threshold<T, IPT, false>, smem))) return r;
         int per_sm = 0;
-        FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_threshold<T, IPT>, T, smem));
+        FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_threshold<T, IPT, false>, T, smem));
         gx = (unsigned)std::min<long long>(2 * g.S, (long long)std::max(1, per_sm) * c->sm_count * 4);
     } else {
-        smem = 0;
-        gx = (unsigned)std::min<long long>(2 * g.S, (long long)c->sm_count * 2);
-        if ((r = bufT(c, "thrwork", work * gx * (size_t)njobs, &gwork))) return r;
+        // global scratch for the runs, sorted values and sweep; the sort's temp
+        // storage in shared memory
+        smem = threshold_sort_tmp_bytes<T, IPT>();
+        if (smem + 8192 > (size_t)c->smem_optin)
+            return fail(FSMELD_E_UNSUPPORTED, "threshold sort does not fit in shared memory");
+        if ((r = allow_smem(c, k_threshold<T, IPT, true>, smem))) return r;
+        int per_sm = 0;
+        FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_threshold<T, IPT, true>, T, smem));
+        gx = (unsigned)std::min<long long>(2 * g.S, (long long)std::max(1, per_sm) * c->sm_count * 2);
+        const size_t gstride = round256(threshold_work_bytes(T * IPT, 0, m));
+        if ((r = bufT(c, "thrwork", gstride * gx * (size_t)njobs, &gwork))) return r;
+        dim3 grid(gx, njobs);
+        prof_begin(c, ST_THR);
+        k_threshold<T, IPT, true><<<grid, T, smem, c->stream>>>(g, djobs, gwork, (long long)gstride);
+        LAUNCH_CHECK(c);
+        return FSMELD_OK;
     }
     dim3 grid(gx, njobs);
     prof_begin(c, ST_THR);
-    k_threshold<T, IPT><<<grid, T, smem, c->stream>>>(g, djobs, gwork, (long long)work);
+    k_threshold<T, IPT, false><<<grid, T, smem, c->stream>>>(g, djobs, gwork, (long long)work);
     LAUNCH_CHECK(c);
     return FSMELD_OK;
 }
@@ -478,9 +497,9 @@ static int run_lbip(fsmeld_ctx* c, const Geom& g, LbJob job) {
     unsigned grid;
     if (smem + 8192 <= (size_t)c->smem_optin) {
         job.gwork = nullptr;
-        if ((r = allow_smem(c, k_lbip<256>, smem))) return r;
+        if ((r = allow_smem(c, k_lbip<256, false>, smem))) return r;
         int per_sm = 0;
-        FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lbip<256>, 256, smem));
+        FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lbip<256, false>, 256, smem));
         grid = (unsigned)std::min<long long>(g.S, (long long)std::max(1, per_sm) * c->sm_count);
     } else {
         grid = (unsigned)std::min<long long>(g.S, (long long)c->sm_count * 2);
@@ -492,7 +511,10 @@ static int run_lbip(fsmeld_ctx* c, const Geom& g, LbJob job) {
         smem = 0;
     }
     prof_begin(c, ST_LBIP);
-    k_lbip<256><<<grid, 256, smem, c->stream>>>(g, job, W, P, logP);
+    if (job.gwork)
+        k_lbip<256, true><<<grid, 256, smem, c->stream>>>(g, job, W, P, logP);
+    else
+        k_lbip<256, false><<<grid, 256, smem, c->stream>>>(g, job, W, P, logP);
     LAUNCH_CHECK(c);
     return FSMELD_OK;
 }

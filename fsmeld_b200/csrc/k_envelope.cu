@@ -183,7 +183,7 @@ __device__ void minmax_phase(const double* __restrict__ src, int n, int par, int
 
 }  // namespace
 
-template <int T, int OPT>
+template <int T, int OPT, bool GW>
 __global__ void __launch_bounds__(T) k_envelope(const double* __restrict__ target,
                                                 const double* __restrict__ MU,
                                                 const double* __restrict__ SIG, Geom g, int w,
@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(T) k_envelope(const double* __restrict__ targe
     extern __shared__ __align__(16) unsigned char env_smem[];
     __shared__ EnvTemp<T> tmp;
     const int mk = g.m_k, kml = g.kml, m = g.m;
-    double* base = gwork ? gwork + (long long)blockIdx.x * slot_stride : (double*)env_smem;
+    double* base = GW ? gwork + (long long)blockIdx.x * slot_stride : (double*)env_smem;
     EnvWork wk;
     wk.raw = base;
     wk.Pmn = base + mk;
@@ -222,9 +222,11 @@ __global__ void __launch_bounds__(T) k_envelope(const double* __restrict__ targe
 
 size_t envelope_work_bytes(int m_k) { return (size_t)m_k * (5 * sizeof(double) + sizeof(int)) + 16; }
 
-#define FSM_ENV_INST(T, OPT)                                                                   \
-    template __global__ void k_envelope<T, OPT>(const double*, const double*, const double*,  \
-                                                Geom, int, double*, double*, double*, long long);
+#define FSM_ENV_INST(T, OPT)                                                                          \
+    template __global__ void k_envelope<T, OPT, false>(const double*, const double*, const double*,  \
+                                                       Geom, int, double*, double*, double*, long long); \
+    template __global__ void k_envelope<T, OPT, true>(const double*, const double*, const double*,   \
+                                                      Geom, int, double*, double*, double*, long long);
 FSM_ENV_INST(128, 8)
 FSM_ENV_INST(256, 8)
 FSM_ENV_INST(512, 8)

@@ -147,7 +147,7 @@ __device__ __forceinline__ unsigned long long bits64(const unsigned long long* w
 
 }  // namespace
 
-template <int T>
+template <int T, bool GW>
 __global__ void __launch_bounds__(T) k_lbip(Geom g, LbJob job, const double2* __restrict__ W, int P,
                                             int logP) {
     using IScan = cub::BlockScan<int, T>;
@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(T) k_lbip(Geom g, LbJob job, const double2* __
     const int tid = threadIdx.x;
     const bool popc_path = (metric == EDR || metric == LCSS);
     const int Pp = P + (P >> 4) + 1;
-    unsigned char* lbase = job.gwork ? job.gwork + (long long)blockIdx.x * job.slot_stride : lb_smem;
+    unsigned char* lbase = GW ? job.gwork + (long long)blockIdx.x * job.slot_stride : lb_smem;
     double2* bufA = (double2*)lbase;
     double2* bufB = bufA + Pp;
     double2* bufC = bufB + Pp;
@@ -334,7 +334,9 @@ int lbip_set_w16() {
     return 0;
 }
 
-template __global__ void k_lbip<256>(Geom, LbJob, const double2*, int, int);
-template __global__ void k_lbip<512>(Geom, LbJob, const double2*, int, int);
+template __global__ void k_lbip<256, false>(Geom, LbJob, const double2*, int, int);
+template __global__ void k_lbip<256, true>(Geom, LbJob, const double2*, int, int);
+template __global__ void k_lbip<512, false>(Geom, LbJob, const double2*, int, int);
+template __global__ void k_lbip<512, true>(Geom, LbJob, const double2*, int, int);
 
 }  // namespace fsm

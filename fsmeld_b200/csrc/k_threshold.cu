@@ -110,7 +110,7 @@ struct Plan {
 
 }  // namespace
 
-template <int T, int IPT>
+template <int T, int IPT, bool GW>
 __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restrict__ jobs,
                                                  unsigned char* gwork, long long slot_stride) {
     using Sort = cub::BlockRadixSort<unsigned long long, T, IPT, int>;
@@ -130,16 +130,23 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
     const int cnt = mk - 2 * m + 2;
     const int t = threadIdx.x;
 
-    unsigned char* base = gwork ? gwork + (long long)(blockIdx.y * gridDim.x + blockIdx.x) * slot_stride
+    // GW: working set in global scratch; otherwise provably shared memory
+    unsigned char* base = GW ? gwork + (long long)(blockIdx.y * gridDim.x + blockIdx.x) * slot_stride
                                 : thr_smem;
     // runs (phases 1-3), then region X: sort temp (phase 2) / sorted values + g (phase 3)
     double* rval = (double*)base;                                          // [CAP]
     int* rstart = (int*)(base + (size_t)CAP * 8);                          // [CAP + 1]
     unsigned char* xb = base + (((size_t)CAP * 12 + 4 + 15) & ~size_t(15));
-    const size_t xbytes = ((sizeof(typename Sort::TempStorage) > (size_t)CAP * 12 + 16
-                                ? sizeof(typename Sort::TempStorage)
-                                : (size_t)CAP * 12 + 16) + 15) & ~size_t(15);
-    typename Sort::TempStorage& sort_tmp = *reinterpret_cast<typename Sort::TempStorage*>(xb);
+    // the sort's temp storage is always in shared memory (cub's block primitives
+    // work on shared memory): in the shared-memory form it shares region X with
+    // the sorted values, in the global-scratch form (GW) it is the block's whole
+    // dynamic shared memory and region X in global memory holds the values only
+    const size_t xbytes = GW ? (((size_t)CAP * 12 + 16 + 15) & ~size_t(15))
+                             : ((sizeof(typename Sort::TempStorage) > (size_t)CAP * 12 + 16
+                                     ? sizeof(typename Sort::TempStorage)
+                                     : (size_t)CAP * 12 + 16) + 15) & ~size_t(15);
+    typename Sort::TempStorage& sort_tmp =
+        *reinterpret_cast<typename Sort::TempStorage*>(GW ? thr_smem : xb);
     double* tv = (double*)xb;                           // [CAP] sorted values
     int* gp = (int*)(xb + (size_t)CAP * 8);             // [CAP] inclusive count sums
     unsigned char* zb = xb + xbytes;
@@ -512,9 +519,11 @@ size_t threshold_sort_tmp_bytes() {
     return sizeof(typename cub::BlockRadixSort<unsigned long long, T, IPT, int>::TempStorage);
 }
 
-#define FSM_THR_INST(T, IPT)                                                              \
-    template __global__ void k_threshold<T, IPT>(Geom, const ThrJob*, unsigned char*,      \
-                                                 long long);                              \
+#define FSM_THR_INST(T, IPT)                                                                 \
+    template __global__ void k_threshold<T, IPT, false>(Geom, const ThrJob*, unsigned char*,  \
+                                                        long long);                          \
+    template __global__ void k_threshold<T, IPT, true>(Geom, const ThrJob*, unsigned char*,   \
+                                                       long long);                           \
     template size_t threshold_sort_tmp_bytes<T, IPT>();
 FSM_THR_INST(128, 4)
 FSM_THR_INST(256, 4)

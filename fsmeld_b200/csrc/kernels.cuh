@@ -77,14 +77,14 @@ struct DpJob {
 
 __global__ void k_mvmean(const double* __restrict__ target, Geom g, double* __restrict__ mu,
                          double* __restrict__ sig);
-template <int T, int OPT>
+template <int T, int OPT, bool GW>
 __global__ void k_envelope(const double* __restrict__ target, const double* __restrict__ MU,
                            const double* __restrict__ SIG, Geom g, int w, double* __restrict__ Un,
                            double* __restrict__ Ln, double* gwork, long long slot_stride);
-template <int T, int IPT>
+template <int T, int IPT, bool GW>
 __global__ void k_threshold(Geom g, const ThrJob* __restrict__ jobs, unsigned char* gwork,
                             long long slot_stride);
-template <int T>
+template <int T, bool GW>
 __global__ void k_lbip(Geom g, LbJob job, const double2* __restrict__ W, int P, int logP);
 template <int METRIC>
 __global__ void k_glb_tq(Geom g, GlbJob job);
