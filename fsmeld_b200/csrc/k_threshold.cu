@@ -9,8 +9,8 @@
 // and a penalty sum C, and scores LB[i] = h(t_i) * g_i; the argmax gives t.
 //
 // Here one CTA handles one (segment, side):
-//  1. dedup with a block scan, sort runs with a block radix sort on an
-//     order-preserving 64-bit key (total order: value, NaN last, ties by
+//  1. dedup with a block scan, sort runs with a stable block merge sort on
+//     an order-preserving 64-bit key (total order: value, NaN last, ties by
 //     position through the sort's stability);
 //  2. every pointer move of the sweep becomes an op with the sweep step at
 //     which it fires (a binary search over the sorted values); ops are
@@ -25,7 +25,7 @@
 // to its heap layout; here equal keys pop by query index.  The threshold is
 // the same unless two candidates' scores tie to the last bit.
 #include <climits>
-#include <cub/block/block_radix_sort.cuh>
+#include <cub/block/block_merge_sort.cuh>
 #include <cub/block/block_reduce.cuh>
 #include <cub/block/block_scan.cuh>
 
@@ -47,6 +47,12 @@ __device__ __forceinline__ unsigned long long order_key(double x, int desc) {
     const unsigned long long k = (u >> 63) ? ~u : (u | 0x8000000000000000ull);
     return desc ? ~k : k;
 }
+
+struct KeyLess {
+    __device__ __forceinline__ bool operator()(const unsigned long long& a, const unsigned long long& b) const {
+        return a < b;
+    }
+};
 
 struct ArgMax {
     double v;
@@ -113,7 +119,7 @@ struct Plan {
 template <int T, int IPT, bool GW>
 __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restrict__ jobs,
                                                  unsigned char* gwork, long long slot_stride) {
-    using Sort = cub::BlockRadixSort<unsigned long long, T, IPT, int>;
+    using Sort = cub::BlockMergeSort<unsigned long long, T, IPT, int>;
     using IScan = cub::BlockScan<int, T>;
     using AReduce = cub::BlockReduce<ArgMax, T>;
     constexpr int CAP = T * IPT;
@@ -206,7 +212,7 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
             keys[k] = (r < nr) ? order_key(rval[r], upper ? 0 : 1) : ~0ull;  // padding after every run
             rid[k] = r;
         }
-        Sort(sort_tmp).Sort(keys, rid);
+        Sort(sort_tmp).StableSort(keys, rid, KeyLess());
         __syncthreads();
 
         // ---- 3. sorted values, cumulative counts g_i, finite prefix length
@@ -388,21 +394,25 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
         const int nops = s_nops;
 
         // ---- 7. replay: initial sums then every op, in the reference's order.
-        // The operands are gathered into shared memory by every thread first,
-        // so the one replaying thread only reads shared memory.
+        // Every thread first gathers the operands into shared memory, already
+        // signed for the accumulator they go to, so that the replaying lanes
+        // only add: x - y is x + (-y) in IEEE arithmetic, and an element or op
+        // that leaves an accumulator unchanged contributes -0.0 (x + -0.0 == x
+        // for every x, signed zeros included).
         const double* pw0 = (kind == 2) ? q.opw : q.pw;
         const double* Dt = (kind == 2) ? q.oD : q.Dq;
-        int* icode = sA;  // kind 2: per query element, 0 skip, 1 power sums, 2 penalty
         for (int j = t; j < m; j += T) {
-            double* o = st + 4 * j;
-            o[0] = pw0[j]; o[1] = pw0[m + j]; o[2] = pw0[2 * m + j]; o[3] = Dt[j];
-            if (kind == 2) {
+            double o0 = pw0[j], o1 = pw0[m + j], o2 = pw0[2 * m + j], o3 = Dt[j];
+            if (kind == 2) {  // which initial sum the element enters, if any
                 const double qv = q.qn[j];
                 int cd;
                 if (!upper) cd = (qv >= t0) ? 0 : (q.otl[j] >= t0 ? 1 : 2);
                 else cd = (qv <= t0) ? 0 : (q.otu[j] <= t0 ? 1 : 2);
-                icode[j] = cd;
+                if (cd != 1) o0 = o1 = o2 = -0.0;
+                if (cd != 2) o3 = -0.0;
             }
+            double* o = st + 4 * j;
+            o[0] = o0; o[1] = o1; o[2] = o2; o[3] = o3;
         }
         __syncthreads();
         // initial sums: lane j of warp 0 owns accumulator j (the power sums
@@ -411,69 +421,93 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
         double acc = 0.0;
         if (t < 4) {
             const int jc = t;
+            // elements e0, e0+dir, ... (len of them); eight operands are loaded
+            // ahead of their adds
+            auto chain = [&](int e0, int dir, int len) {
+                for (int i0 = 0; i0 < len; i0 += 8) {
+                    double v[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        const int i = i0 + u;
+                        v[u] = (i < len) ? st[4 * (e0 + dir * i) + jc] : 0.0;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+                        if (i0 + u < len) acc = dadd(acc, v[u]);
+                }
+            };
             if (jc < 3) {
                 if (kind == 0) {
-                    if (!upper) { for (int e = 0; e <= pl.idx1; ++e) acc = dadd(acc, st[4 * e + jc]); }
-                    else { for (int e = pl.idx1; e < m; ++e) acc = dadd(acc, st[4 * e + jc]); }
+                    if (!upper) chain(0, 1, pl.idx1 + 1);
+                    else chain(pl.idx1, 1, m - pl.idx1);
                 } else if (kind == 1) {
-                    if (!upper) { for (int e = pl.idx1; e > pl.idx2; --e) acc = dadd(acc, st[4 * e + jc]); }
-                    else { for (int e = pl.idx1; e < pl.idx2; ++e) acc = dadd(acc, st[4 * e + jc]); }
+                    if (!upper) chain(pl.idx1, -1, pl.idx1 - pl.idx2);
+                    else chain(pl.idx1, 1, pl.idx2 - pl.idx1);
                 } else {
-                    for (int e = 0; e < m; ++e)
-                        if (icode[e] == 1) acc = dadd(acc, st[4 * e + jc]);
+                    chain(0, 1, m);
                 }
             } else {
                 if (kind == 1) {
-                    if (!upper) { for (int e = 0; e <= pl.idx2; ++e) acc = dadd(acc, st[4 * e + 3]); }
-                    else { for (int e = pl.idx2; e < m; ++e) acc = dadd(acc, st[4 * e + 3]); }
+                    if (!upper) chain(0, 1, pl.idx2 + 1);
+                    else chain(pl.idx2, 1, m - pl.idx2);
                 } else if (kind == 2) {
-                    for (int e = 0; e < m; ++e)
-                        if (icode[e] == 2) acc = dadd(acc, st[4 * e + 3]);
+                    chain(0, 1, m);
                 }
             }
         }
         __syncthreads();
-        // op payloads into the state slots the replay overwrites
+        // op payloads into the state slots the replay overwrites: op B
+        // subtracts the element's powers, op A adds them and subtracts its
+        // penalty
         for (int k = t; k < nops; k += T) {
             const int d = opdesc[k];
             double* o = st + 4 * (k + 1);
             if (d < 0) {  // unreachable when the op order is a permutation; keeps reads in bounds
-                o[0] = o[1] = o[2] = o[3] = 0.0;
+                o[0] = o[1] = o[2] = o[3] = -0.0;
                 continue;
             }
             const int r = d & 0x3fffffff;
+            const bool op_b = (d & 0x40000000) != 0;
             int x;  // table index of the op's query element
-            if (kind == 2) x = (d & 0x40000000) ? (upper ? q.ordB_u : q.ordB_l)[pl.kB0 + r]
-                                                : (upper ? q.ordA_u : q.ordA_l)[pl.kA0 + r];
-            else if (d & 0x40000000) x = upper ? pl.idx1 + r : pl.idx1 - r;
+            if (kind == 2) x = op_b ? (upper ? q.ordB_u : q.ordB_l)[pl.kB0 + r]
+                                    : (upper ? q.ordA_u : q.ordA_l)[pl.kA0 + r];
+            else if (op_b) x = upper ? pl.idx1 + r : pl.idx1 - r;
             else x = upper ? pl.idx2 + r : pl.idx2 - r;
             x = min(max(x, 0), m - 1);
-            o[0] = pw0[x]; o[1] = pw0[m + x]; o[2] = pw0[2 * m + x]; o[3] = Dt[x];
+            const double a0 = pw0[x], a1 = pw0[m + x], a2 = pw0[2 * m + x], a3 = Dt[x];
+            o[0] = op_b ? -a0 : a0;
+            o[1] = op_b ? -a1 : a1;
+            o[2] = op_b ? -a2 : a2;
+            o[3] = op_b ? -0.0 : -a3;
         }
         __syncthreads();
-        // replay: lane j applies every op to its accumulator j (op B
-        // subtracts the element's powers; op A adds them and subtracts its
-        // penalty), storing the state after each op
+        // replay: lane j adds every op's operand to its accumulator j and
+        // stores the state after each op, in chunks of eight (the next chunk's
+        // operands are loaded before this chunk's states overwrite its slots)
         if (t < 4) {
             const int jc = t;
             st[jc] = acc;
-            double* o = st + 4 + jc;
-            double a = 0.0;
-            int d = 0;
-            if (nops > 0) { a = o[0]; d = opdesc[0]; }
-            for (int k = 0; k < nops; ++k, o += 4) {
-                // next op's operand before this op's state overwrites its slot
-                double na = 0.0;
-                int nd = 0;
-                if (k + 1 < nops) { na = o[4]; nd = opdesc[k + 1]; }
-                if (d >= 0) {
-                    const bool op_b = (d & 0x40000000) != 0;
-                    const double sub = dsub(acc, a), add = dadd(acc, a);
-                    acc = (jc < 3) ? (op_b ? sub : add) : (op_b ? acc : sub);
+            constexpr int RC = 8;
+            double a[RC];
+#pragma unroll
+            for (int u = 0; u < RC; ++u) a[u] = (u < nops) ? st[4 * (u + 1) + jc] : 0.0;
+            for (int k0 = 0; k0 < nops; k0 += RC) {
+                double na[RC];
+#pragma unroll
+                for (int u = 0; u < RC; ++u) {
+                    const int k = k0 + RC + u;
+                    na[u] = (k < nops) ? st[4 * (k + 1) + jc] : 0.0;
                 }
-                o[0] = acc;
-                a = na;
-                d = nd;
+#pragma unroll
+                for (int u = 0; u < RC; ++u) {
+                    const int k = k0 + u;
+                    if (k < nops) {
+                        acc = dadd(acc, a[u]);
+                        st[4 * (k + 1) + jc] = acc;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < RC; ++u) a[u] = na[u];
             }
         }
         __syncthreads();
@@ -481,9 +515,17 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
         // ---- 8. scores and first maximum
         ArgMax best{0.0, INT_MAX, 0};
         int nan0 = 0;
-        for (int i = t; i < nr; i += T) {
-            int lo = 0, hi = nops;  // ops with step <= i
-            while (lo < hi) { const int mid = (lo + hi) >> 1; if (opstep[mid] <= i) lo = mid + 1; else hi = mid; }
+        // each thread scores a contiguous range of steps, so the number of ops
+        // with step <= i is one binary search followed by a forward walk
+        const int per = (nr + T - 1) / T;
+        const int i_beg = t * per, i_end = min(i_beg + per, nr);
+        int lo = 0;
+        if (i_beg < i_end) {
+            int hi = nops;
+            while (lo < hi) { const int mid = (lo + hi) >> 1; if (opstep[mid] <= i_beg) lo = mid + 1; else hi = mid; }
+        }
+        for (int i = i_beg; i < i_end; ++i) {
+            while (lo < nops && opstep[lo] <= i) ++lo;
             const double* sv = st + 4 * lo;
             const double tt = tv[i];
             const double f = f_p(sv[0], sv[1], sv[2], p, tt);
@@ -516,7 +558,7 @@ size_t threshold_work_bytes(int cap_items, size_t sort_tmp, int m) {
 
 template <int T, int IPT>
 size_t threshold_sort_tmp_bytes() {
-    return sizeof(typename cub::BlockRadixSort<unsigned long long, T, IPT, int>::TempStorage);
+    return sizeof(typename cub::BlockMergeSort<unsigned long long, T, IPT, int>::TempStorage);
 }
 
 #define FSM_THR_INST(T, IPT)                                                                 \
