@@ -116,8 +116,19 @@ struct Plan {
 
 }  // namespace
 
+// Block working set: the runs (values and starts), region X (the sort's temp
+// storage, then the sorted values and counts) and region Z (the sweep: op
+// steps, op order, operand/state slots).  Z is used only after the runs are
+// dead, so it lives in the runs region whenever it fits there (segments of at
+// least 8m points, the usual case).
+__host__ __device__ inline size_t thr_runs_bytes(int cap) { return ((size_t)cap * 12 + 4 + 15) & ~size_t(15); }
+__host__ __device__ inline size_t thr_z_bytes(int m) { return (size_t)m * 24 + 16 + (size_t)(2 * m + 1) * 32; }
+__host__ __device__ inline bool thr_z_in_runs(int cap, int m) { return thr_z_bytes(m) <= thr_runs_bytes(cap); }
+
+// 1024 / T blocks per SM: at most 64 registers a thread, so that several
+// blocks hide each other's serial phases
 template <int T, int IPT, bool GW>
-__global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restrict__ jobs,
+__global__ void __launch_bounds__(T, 1024 / T) k_threshold(Geom g, const ThrJob* __restrict__ jobs,
                                                  unsigned char* gwork, long long slot_stride) {
     using Sort = cub::BlockMergeSort<unsigned long long, T, IPT, int>;
     using IScan = cub::BlockScan<int, T>;
@@ -142,7 +153,7 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
     // runs (phases 1-3), then region X: sort temp (phase 2) / sorted values + g (phase 3)
     double* rval = (double*)base;                                          // [CAP]
     int* rstart = (int*)(base + (size_t)CAP * 8);                          // [CAP + 1]
-    unsigned char* xb = base + (((size_t)CAP * 12 + 4 + 15) & ~size_t(15));
+    unsigned char* xb = base + thr_runs_bytes(CAP);
     // the sort's temp storage is always in shared memory (cub's block primitives
     // work on shared memory): in the shared-memory form it shares region X with
     // the sorted values, in the global-scratch form (GW) it is the block's whole
@@ -155,7 +166,7 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
         *reinterpret_cast<typename Sort::TempStorage*>(GW ? thr_smem : xb);
     double* tv = (double*)xb;                           // [CAP] sorted values
     int* gp = (int*)(xb + (size_t)CAP * 8);             // [CAP] inclusive count sums
-    unsigned char* zb = xb + xbytes;
+    unsigned char* zb = thr_z_in_runs(CAP, m) ? base : xb + xbytes;
     int* sA = (int*)zb;                                 // [m]
     int* sB = sA + m;                                   // [m]
     int* opdesc = sB + m;                               // [2m]
@@ -550,9 +561,9 @@ __global__ void __launch_bounds__(T) k_threshold(Geom g, const ThrJob* __restric
 
 size_t threshold_work_bytes(int cap_items, size_t sort_tmp, int m) {
     const size_t cap = (size_t)cap_items;
-    const size_t runs = (cap * 12 + 4 + 15) & ~size_t(15);
+    const size_t runs = thr_runs_bytes(cap_items);
     const size_t x = ((sort_tmp > cap * 12 + 16 ? sort_tmp : cap * 12 + 16) + 15) & ~size_t(15);
-    const size_t z = (size_t)m * 4 * 6 + 16 + (size_t)(2 * m + 1) * 4 * 8;
+    const size_t z = thr_z_in_runs(cap_items, m) ? 0 : thr_z_bytes(m);
     return runs + x + z + 64;
 }
 
