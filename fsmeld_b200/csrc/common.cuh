@@ -10,6 +10,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "rcpdiv.h"
+
 namespace fsm {
 
 constexpr double kDpMax = 1e18;                     // src/ElasticMeasures.cpp:7
@@ -26,6 +28,14 @@ __device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a,
 __device__ __forceinline__ double dsqrt(double a) { return __dsqrt_rn(a); }
 __device__ __forceinline__ double dnan() { return __longlong_as_double(0x7ff8000000000000LL); }
 __device__ __forceinline__ double dsq(double a, double b) { double d = dsub(a, b); return dmul(d, d); }
+// a / sg correctly rounded, from inv = RN(1/sg): the reciprocal and two FMA
+// corrections of rcpdiv.h when sg (ok) and the quotient estimate are in that
+// method's range, a division otherwise -- the same bits either way
+__device__ __forceinline__ double zdiv(double a, double sg, double inv, bool ok) {
+    const double q0 = rcp_div_estimate(a, inv);
+    if (ok && rcp_div_in_range(q0)) return rcp_div_finish(a, sg, inv, q0);
+    return ddiv(a, sg);
+}
 // std::max(0.0, x): (0.0 < x) ? x : 0.0 (a NaN x gives 0.0)
 __device__ __forceinline__ double dmax0(double x) { return (0.0 < x) ? x : 0.0; }
 // std::min({a, b, c}) for non-NaN operands
@@ -100,9 +110,9 @@ __device__ __forceinline__ int qt_p1(int k, int m, int w) { return k < m - 1 - w
 
 // The term from the raw window minimum a and maximum b of the candidate at k.
 __device__ __forceinline__ double qt_term_env(int metric, double x, double a, double b, double mu, double sg,
-                                              double arg) {
-    const double lo = ddiv(dsub(a, mu), sg);
-    const double up = ddiv(dsub(b, mu), sg);
+                                              double inv, bool ok, double arg) {
+    const double lo = zdiv(dsub(a, mu), sg, inv, ok);
+    const double up = zdiv(dsub(b, mu), sg, inv, ok);
     switch (metric) {
         case DTW:
             if (x < lo) return dsq(x, lo);
@@ -165,11 +175,12 @@ __device__ __forceinline__ double qt_term_bound(int metric, double x, double a, 
 }
 
 __device__ __forceinline__ double qt_term(int metric, double x, int k, int m, int w, const double* lf,
-                                          const double* uf, double mu, double sg, double arg) {
+                                          const double* uf, double mu, double sg, double inv, bool ok,
+                                          double arg) {
     const int p0 = qt_p0(k, w), p1 = qt_p1(k, m, w);
     // valid windows hold no NaN: a comparison and a select give the min / max
     const double a0 = lf[p0], a1 = lf[p1], b0 = uf[p0], b1 = uf[p1];
-    return qt_term_env(metric, x, (a1 < a0) ? a1 : a0, (b0 < b1) ? b1 : b0, mu, sg, arg);
+    return qt_term_env(metric, x, (a1 < a0) ? a1 : a0, (b0 < b1) ? b1 : b0, mu, sg, inv, ok, arg);
 }
 
 // Per-query tables prepared on the host (query z-normalisation as

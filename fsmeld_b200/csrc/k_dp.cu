@@ -227,6 +227,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
     const double* lr = job.lraw;
     const double* ur = job.uraw;
     double mu = 0.0, sg = 1.0, inv = 1.0;
+    bool rok = false;  // sg in the range of the reciprocal division (zdiv)
     int row = 0, ny = 0;
     double Ssum = 0.0, Pre = 0.0;  // GLB Q->T sum of the candidate, and its prefix over rows done
     bool has_s = false;
@@ -252,7 +253,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
         for (; ny <= upto; ++ny) {
             double y = kPad;
             if (ny < m) {
-                y = ddiv(dsub(ny == nty ? nt : tp[ny], mu), sg);
+                y = zdiv(dsub(ny == nty ? nt : tp[ny], mu), sg, inv, rok);
                 over = over || !(fabs(y) <= ylim);
             }
             R[(ny & RM) * 32] = y;
@@ -328,6 +329,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
                     if (!window_invalid(sg, g, gi)) {
                         tp = job.target + gi;
                         inv = ddiv(1.0, sg);
+                        rok = rcp_div_in_range(sg);
                         if (job.lraw) { lr = job.lraw + gi; ur = job.uraw + gi; }
                         ++valid_count;
                         has_s = job.list_s && job.lraw && job.list_s[c] >= 0.0;
@@ -348,6 +350,8 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
                 const double* tpL = (const double*)__shfl_sync(0xffffffffu, (unsigned long long)tp, L);
                 const double muL = __shfl_sync(0xffffffffu, mu, L);
                 const double sgL = __shfl_sync(0xffffffffu, sg, L);
+                const double invL = __shfl_sync(0xffffffffu, inv, L);
+                const bool rokL = __shfl_sync(0xffffffffu, (int)rok, L) != 0;
                 double* AL = wbase + L;
                 double* RL = wbase + (size_t)(W2 + 1) * 32 + L;
                 for (int d = lane; d <= W2; d += 32) {
@@ -364,7 +368,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
                 for (int c = lane; c <= w; c += 32) {
                     double y = kPad;
                     if (c < m) {
-                        y = ddiv(dsub(tpL[c], muL), sgL);
+                        y = zdiv(dsub(tpL[c], muL), sgL, invL, rokL);
                         bad = bad || !(fabs(y) <= ylim);
                     }
                     RL[(c & RM) * 32] = y;

@@ -2,8 +2,9 @@
 // directions:
 //  * k_glb_tq: one lane per LB_IP survivor computes the boundary term and the
 //    T->Q sum with early abandon, z-normalising candidate points lazily
-//    (t - mu) / sigma exactly as src/fsmeld.cpp:823-826 does, so abandoned
-//    candidates never pay for the whole window;
+//    (t - mu) / sigma exactly as src/fsmeld.cpp:823-826 does (one correctly
+//    rounded division, taken from the window's reciprocal by FMA corrections),
+//    so abandoned candidates never pay for the whole window;
 //  * k_glb_qt: one lane per T->Q survivor adds the Q->T terms in the
 //    reference's order.  The candidate envelope (lower_upper_lemire of the
 //    z-normalised window, src/glb.cpp:302-304) is never materialised:
@@ -87,7 +88,7 @@ __global__ void __launch_bounds__(256) k_glb_tq(Geom g, GlbJob job) {
         const unsigned long long idx = base + threadIdx.x;
         const bool active = idx < n_lim;
         long long gi = 0;
-        double mu = 0.0, sg = 1.0;
+        double mu = 0.0, sg = 1.0, inv = 1.0;
         if (active) {
             gi = job.in[idx];
             long long s;
@@ -95,12 +96,14 @@ __global__ void __launch_bounds__(256) k_glb_tq(Geom g, GlbJob job) {
             g.locate(gi, &s, &j);
             mu = job.MU[s * g.kml + j];
             sg = job.SIG[s * g.kml + j];
+            inv = __drcp_rn(sg);
         }
+        const bool rok = rcp_div_in_range(sg);
         const double* tp = job.target + gi;
         bool alive = active;
         double boundary = 0.0, tq = 0.0;
         if (active) {
-#define TN(k) ddiv(dsub(tp[(k)], mu), sg)
+#define TN(k) zdiv(dsub(tp[(k)], mu), sg, inv, rok)
             const double T0 = TN(0), TL = TN(m - 1);
             if (METRIC == DTW) {
                 boundary = dadd(dsq(T0, Q[0]), dsq(TL, Q[m - 1]));
@@ -215,13 +218,15 @@ __global__ void __launch_bounds__(128) k_glb_qt(Geom g, GlbJob job) {
             glb = kGlbMax;  // abandoned in T->Q but MAX_VAL <= cutoff
         } else {
             const double mu = job.MU[s * g.kml + j], sg = job.SIG[s * g.kml + j];
+            const double inv = __drcp_rn(sg);
+            const bool rok = rcp_div_in_range(sg);
             const double* lf = job.lraw + gi;
             const double* uf = job.uraw + gi;
             const int k0 = (METRIC == LCSS) ? 0 : 1, k1 = (METRIC == LCSS) ? m - 1 : m - 2;
             // the terms are independent (unrolled so their loads and divisions
             // overlap); only the sum is sequential, in the reference's order
 #pragma unroll 4
-            for (int k = k0; k <= k1; ++k) qt = dadd(qt, qt_term(METRIC, Q[k], k, m, w, lf, uf, mu, sg, arg));
+            for (int k = k0; k <= k1; ++k) qt = dadd(qt, qt_term(METRIC, Q[k], k, m, w, lf, uf, mu, sg, inv, rok, arg));
             if (METRIC == LCSS) {
                 glb = dmax0(dsub(1.0, ddiv(dminv(tq, qt), (double)m)));
             } else {

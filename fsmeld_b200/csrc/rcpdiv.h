@@ -19,10 +19,8 @@
 // IEEE division) and as CUDA device code.
 #pragma once
 
-#if defined(__CUDA_ARCH__)
-#define FSM_RD_HD __device__ __forceinline__
-#define FSM_RD_MUL(a, b) __dmul_rn((a), (b))
-#define FSM_RD_FMA(a, b, c) __fma_rn((a), (b), (c))
+#if defined(__CUDACC__)
+#define FSM_RD_HD __host__ __device__ __forceinline__
 #else
 #include <math.h>
 #if defined(__cplusplus)
@@ -30,9 +28,23 @@
 #else
 #define FSM_RD_HD static inline
 #endif
-#define FSM_RD_MUL(a, b) ((a) * (b))
-#define FSM_RD_FMA(a, b, c) fma((a), (b), (c))
 #endif
+
+// round-to-nearest product and fused multiply-add, never contracted
+FSM_RD_HD double rcp_div_mul(double a, double b) {
+#if defined(__CUDA_ARCH__)
+    return __dmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+FSM_RD_HD double rcp_div_fma(double a, double b, double c) {
+#if defined(__CUDA_ARCH__)
+    return __fma_rn(a, b, c);
+#else
+    return fma(a, b, c);
+#endif
+}
 
 // |x| in [2^-450, 2^450] (false for zero, subnormals, infinities and NaN)
 FSM_RD_HD int rcp_div_in_range(double x) {
@@ -42,11 +54,11 @@ FSM_RD_HD int rcp_div_in_range(double x) {
 
 // RN(a / b) from y = RN(1 / b); the caller has checked rcp_div_in_range(b)
 // and rcp_div_in_range(q0), q0 = rcp_div_estimate(a, y)
-FSM_RD_HD double rcp_div_estimate(double a, double y) { return FSM_RD_MUL(a, y); }
+FSM_RD_HD double rcp_div_estimate(double a, double y) { return rcp_div_mul(a, y); }
 
 FSM_RD_HD double rcp_div_finish(double a, double b, double y, double q0) {
-    const double r0 = FSM_RD_FMA(-q0, b, a);
-    const double q1 = FSM_RD_FMA(r0, y, q0);
-    const double r1 = FSM_RD_FMA(-q1, b, a);
-    return FSM_RD_FMA(r1, y, q1);
+    const double r0 = rcp_div_fma(-q0, b, a);
+    const double q1 = rcp_div_fma(r0, y, q0);
+    const double r1 = rcp_div_fma(-q1, b, a);
+    return rcp_div_fma(r1, y, q1);
 }

@@ -324,3 +324,27 @@ def test_cutoff_k_larger_than_segments(api, oracle):
                 gidx, gdist, _ = e.cutoff(q, m, k, metric, w, arg)
                 oidx, odist, _ = oracle.cutoff(t, q, m, k, metric, w, arg)
                 assert list(gidx) == list(oidx) and bits_equal(gdist, odist), (metric, k)
+
+
+@pytest.mark.parametrize("scale", [1.0, 1e-5, 1e140])
+def test_division_paths_vs_oracle(api, oracle, scale):
+    # candidate z-normalisation divides by the window's sigma through its
+    # reciprocal (reciprocal, two FMA corrections) unless the sigma or the
+    # quotient lies outside [2^-450, 2^450]: an integer-valued walk has points
+    # equal to their window mean (zero dividends), and at scale 1e140 every
+    # sigma is past 2^450 so every division takes the direct path
+    rng = np.random.default_rng(17)
+    m, w = 64, 4
+    t = np.cumsum(rng.integers(-2, 3, 1 << 14)).astype(np.float64) * scale
+    q, _ = query_from(t, m, np.random.default_rng(5))
+    with api.Engine(t) as e:
+        for metric, arg in [("dtw", 0.0), ("erp", 0.3), ("lcss", 0.25), ("msm", 0.5)]:
+            gidx, gdist, _ = e.exact(q, m, 1e300, metric, w, arg)
+            oidx, odist, _ = oracle.exact(t, q, m, 1e300, metric, w, arg)
+            assert list(gidx) == list(oidx) and bits_equal(gdist, odist), metric
+            kidx, kdist, _ = oracle.cutoff(t, q, m, 20, metric, w, arg)
+            cut = float(kdist[-1])
+            sidx, sc = e.search(q, m, cut, metric, w, arg)
+            xidx, xc = oracle.search(t, q, m, cut, metric, w, arg)
+            assert list(sidx) == list(xidx), metric
+            assert (sc["after_lb"], sc["after_glb"]) == (xc["after_lb"], xc["after_glb"]), metric
