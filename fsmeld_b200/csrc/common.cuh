@@ -36,6 +36,12 @@ __device__ __forceinline__ double zdiv(double a, double sg, double inv, bool ok)
     if (ok && rcp_div_in_range(q0)) return rcp_div_finish(a, sg, inv, q0);
     return ddiv(a, sg);
 }
+// zdiv with the estimate's range tested on the integer pipe
+__device__ __forceinline__ double zdiv_i(double a, double sg, double inv, bool ok) {
+    const double q0 = rcp_div_estimate(a, inv);
+    if (ok && rcp_div_in_range_bits(q0)) return rcp_div_finish(a, sg, inv, q0);
+    return ddiv(a, sg);
+}
 // std::max(0.0, x): (0.0 < x) ? x : 0.0 (a NaN x gives 0.0)
 __device__ __forceinline__ double dmax0(double x) { return (0.0 < x) ? x : 0.0; }
 // std::min({a, b, c}) for non-NaN operands

@@ -44,31 +44,33 @@ __device__ __forceinline__ void warp_append(bool pred, unsigned long long* count
 }  // namespace
 
 // T->Q term of normalised candidate point t against the query envelope
-// [lo, hi] at the same index (src/glb.cpp:230-300), written with selects: both
-// sides are computed and one is chosen, so lanes never split on the data.
+// [lo, hi] at the same index (src/glb.cpp:230-300), written with selects so
+// lanes never split on the data.  lo <= hi, so at most one of t < lo, t > hi
+// holds: the side is selected first and one distance computed to it.
 template <int METRIC>
 __device__ __forceinline__ double tq_term(double t, double lo, double hi, double arg) {
+    const bool below = t < lo, above = t > hi;
+    const double e = above ? hi : lo;  // the nearer side when outside
     if (METRIC == DTW) {
-        const double a = dsq(t, lo), b = dsq(t, hi);
-        return (t < lo) ? a : ((t > hi) ? b : 0.0);
+        const double a = dsq(t, e);
+        return (below || above) ? a : 0.0;
     } else if (METRIC == ERP) {
-        const double g2 = dsq(t, arg);
-        const double a = dminv(dsq(t, hi), g2), b = dminv(dsq(t, lo), g2);
-        return (t > hi) ? a : ((t < lo) ? b : 0.0);
+        const double a = dminv(dsq(t, e), dsq(t, arg));
+        return (below || above) ? a : 0.0;
     } else if (METRIC == EDR) {
-        const double a = edr_sub(t, hi, arg), b = edr_sub(t, lo, arg);
-        return (t > hi) ? a : ((t < lo) ? b : 0.0);
-    } else if (METRIC == LCSS) {  // match indicator
-        const bool a = dsub(lo, t) <= arg, b = dsub(t, hi) <= arg;
-        return ((t < lo) ? a : ((t > hi) ? b : true)) ? 1.0 : 0.0;
+        const double a = edr_sub(t, e, arg);
+        return (below || above) ? a : 0.0;
+    } else if (METRIC == LCSS) {  // match indicator: lo - t or t - hi within eps
+        const bool a = dsub(below ? lo : t, below ? t : hi) <= arg;
+        return ((below || above) ? a : true) ? 1.0 : 0.0;
     } else {  // MSM
-        const double a = dminv(fabs(dsub(t, hi)), arg), b = dminv(fabs(dsub(t, lo)), arg);
-        return (t > hi) ? a : ((t < lo) ? b : 0.0);
+        const double a = dminv(fabs(dsub(t, e)), arg);
+        return (below || above) ? a : 0.0;
     }
 }
 
 template <int METRIC>
-__global__ void __launch_bounds__(256) k_glb_tq(Geom g, GlbJob job) {
+__global__ void __launch_bounds__(256, 5) k_glb_tq(Geom g, GlbJob job) {
     extern __shared__ double gq_smem[];
     const QueryDev& q = job.q;
     const int m = q.m;
@@ -103,7 +105,7 @@ __global__ void __launch_bounds__(256) k_glb_tq(Geom g, GlbJob job) {
         bool alive = active;
         double boundary = 0.0, tq = 0.0;
         if (active) {
-#define TN(k) zdiv(dsub(tp[(k)], mu), sg, inv, rok)
+#define TN(k) zdiv_i(dsub(tp[(k)], mu), sg, inv, rok)
             const double T0 = TN(0), TL = TN(m - 1);
             if (METRIC == DTW) {
                 boundary = dadd(dsq(T0, Q[0]), dsq(TL, Q[m - 1]));

@@ -20,9 +20,11 @@
 #pragma once
 
 #if defined(__CUDACC__)
+#include <string.h>
 #define FSM_RD_HD __host__ __device__ __forceinline__
 #else
 #include <math.h>
+#include <string.h>
 #if defined(__cplusplus)
 #define FSM_RD_HD inline
 #else
@@ -46,10 +48,26 @@ FSM_RD_HD double rcp_div_fma(double a, double b, double c) {
 #endif
 }
 
-// |x| in [2^-450, 2^450] (false for zero, subnormals, infinities and NaN)
+// |x| in [2^-450, 2^450] (false for zero, subnormals, infinities and NaN),
+// two floating-point comparisons
 FSM_RD_HD int rcp_div_in_range(double x) {
     const double ax = fabs(x);
     return ax >= 0x1p-450 && ax <= 0x1p+450;
+}
+
+// The same test on the integer pipe, for kernels whose floating-point pipe
+// is the busier one: |x| in [2^-450, 2^450) from the biased exponent field e,
+// 1023 - 450 <= e < 1023 + 450 (implies rcp_div_in_range(x))
+FSM_RD_HD int rcp_div_in_range_bits(double x) {
+#if defined(__CUDA_ARCH__)
+    const unsigned hi = (unsigned)__double2hiint(x);
+#else
+    unsigned long long u;
+    memcpy(&u, &x, 8);
+    const unsigned hi = (unsigned)(u >> 32);
+#endif
+    const unsigned e = (hi >> 20) & 0x7ffu;
+    return e - 573u < 900u;
 }
 
 // RN(a / b) from y = RN(1 / b); the caller has checked rcp_div_in_range(b)
