@@ -226,9 +226,19 @@ __global__ void __launch_bounds__(128) k_glb_qt(Geom g, GlbJob job) {
             const double* uf = job.uraw + gi;
             const int k0 = (METRIC == LCSS) ? 0 : 1, k1 = (METRIC == LCSS) ? m - 1 : m - 2;
             // the terms are independent (unrolled so their loads and divisions
-            // overlap); only the sum is sequential, in the reference's order
+            // overlap); only the sum is sequential, in the reference's order.
+            // Interior points (w <= k <= m-1-w) read the windows at k-w and k
+            // directly; the edges take the clamped indices.
+            const int i0 = max(k0, w), i1 = min(k1, m - 1 - w);
+            int k = k0;
+            for (; k <= k1 && k < i0; ++k) qt = dadd(qt, qt_term(METRIC, Q[k], k, m, w, lf, uf, mu, sg, inv, rok, arg));
 #pragma unroll 4
-            for (int k = k0; k <= k1; ++k) qt = dadd(qt, qt_term(METRIC, Q[k], k, m, w, lf, uf, mu, sg, inv, rok, arg));
+            for (; k <= i1; ++k) {
+                const double a0 = lf[k - w], a1 = lf[k], b0 = uf[k - w], b1 = uf[k];
+                qt = dadd(qt, qt_term_env(METRIC, Q[k], (a1 < a0) ? a1 : a0, (b0 < b1) ? b1 : b0, mu, sg, inv, rok,
+                                          arg));
+            }
+            for (; k <= k1; ++k) qt = dadd(qt, qt_term(METRIC, Q[k], k, m, w, lf, uf, mu, sg, inv, rok, arg));
             if (METRIC == LCSS) {
                 glb = dmax0(dsub(1.0, ddiv(dminv(tq, qt), (double)m)));
             } else {
