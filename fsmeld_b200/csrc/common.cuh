@@ -115,10 +115,8 @@ __device__ __forceinline__ int qt_p0(int k, int w) { return k - w < 0 ? 0 : k - 
 __device__ __forceinline__ int qt_p1(int k, int m, int w) { return k < m - 1 - w ? k : m - 1 - w; }
 
 // The term from the raw window minimum a and maximum b of the candidate at k.
-__device__ __forceinline__ double qt_term_env(int metric, double x, double a, double b, double mu, double sg,
-                                              double inv, bool ok, double arg) {
-    const double lo = zdiv(dsub(a, mu), sg, inv, ok);
-    const double up = zdiv(dsub(b, mu), sg, inv, ok);
+// The term from the normalised envelope [lo, up] of the candidate at k.
+__device__ __forceinline__ double qt_term_norm(int metric, double x, double lo, double up, double arg) {
     switch (metric) {
         case DTW:
             if (x < lo) return dsq(x, lo);
@@ -141,6 +139,11 @@ __device__ __forceinline__ double qt_term_env(int metric, double x, double a, do
             if (x < lo) { const double p = fabs(dsub(x, lo)); return (p < arg) ? p : arg; }
             return 0.0;
     }
+}
+
+__device__ __forceinline__ double qt_term_env(int metric, double x, double a, double b, double mu, double sg,
+                                              double inv, bool ok, double arg) {
+    return qt_term_norm(metric, x, zdiv(dsub(a, mu), sg, inv, ok), zdiv(dsub(b, mu), sg, inv, ok), arg);
 }
 
 // The same term for the DP's cascading abandon test, without divisions: the

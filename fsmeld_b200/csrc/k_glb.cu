@@ -41,6 +41,27 @@ __device__ __forceinline__ void warp_append(bool pred, unsigned long long* count
     if (pred) write(base + __popc(mask & ((1u << lane) - 1)));
 }
 
+// N quotients dividend(u) / sg (zdiv) with one range test for the group: a
+// group with any estimate outside the reciprocal method's range (zero
+// dividends, extreme scales) is divided directly -- the same bits either way,
+// one branch per group instead of one per point.  The rare direct path
+// evaluates the dividends again rather than keeping them live.
+template <int N, typename F>
+__device__ __forceinline__ void zdiv_group(F dividend, double sg, double inv, bool ok, double (&z)[N]) {
+    bool good = ok;
+#pragma unroll
+    for (int u = 0; u < N; ++u) {
+        const double a = dividend(u);
+        const double q0 = rcp_div_estimate(a, inv);
+        good = good & (rcp_div_in_range_bits(q0) != 0);
+        z[u] = rcp_div_finish(a, sg, inv, q0);
+    }
+    if (!good) {
+#pragma unroll
+        for (int u = 0; u < N; ++u) z[u] = ddiv(dividend(u), sg);
+    }
+}
+
 }  // namespace
 
 // T->Q term of normalised candidate point t against the query envelope
@@ -70,7 +91,7 @@ __device__ __forceinline__ double tq_term(double t, double lo, double hi, double
 }
 
 template <int METRIC>
-__global__ void __launch_bounds__(256, 5) k_glb_tq(Geom g, GlbJob job) {
+__global__ void __launch_bounds__(256, 4) k_glb_tq(Geom g, GlbJob job) {
     extern __shared__ double gq_smem[];
     const QueryDev& q = job.q;
     const int m = q.m;
@@ -130,9 +151,10 @@ __global__ void __launch_bounds__(256, 5) k_glb_tq(Geom g, GlbJob job) {
                 const double min_len = (double)m;
                 int k = 0;
                 for (; k + 4 <= m; k += 4) {
-                    double t4[4];
+                    double z4[4], t4[4];
+                    zdiv_group([&](int u) { return dsub(tp[k + u], mu); }, sg, inv, rok, z4);
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) t4[u] = tq_term<LCSS>(TN(k + u), LQ[k + u], UQ[k + u], arg);
+                    for (int u = 0; u < 4; ++u) t4[u] = tq_term<LCSS>(z4[u], LQ[k + u], UQ[k + u], arg);
 #pragma unroll
                     for (int u = 0; u < 4; ++u) tq = dadd(tq, t4[u]);
                 }
@@ -146,9 +168,10 @@ __global__ void __launch_bounds__(256, 5) k_glb_tq(Geom g, GlbJob job) {
                 // past it at the group's end (the same decision)
                 int k = 1;
                 for (; k + 4 <= m - 1; k += 4) {
-                    double t4[4];
+                    double z4[4], t4[4];
+                    zdiv_group([&](int u) { return dsub(tp[k + u], mu); }, sg, inv, rok, z4);
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) t4[u] = tq_term<METRIC>(TN(k + u), LQ[k + u], UQ[k + u], arg);
+                    for (int u = 0; u < 4; ++u) t4[u] = tq_term<METRIC>(z4[u], LQ[k + u], UQ[k + u], arg);
 #pragma unroll
                     for (int u = 0; u < 4; ++u) tq = dadd(tq, t4[u]);
                     if (dadd(boundary, tq) > lim) { alive = false; break; }
@@ -232,7 +255,19 @@ __global__ void __launch_bounds__(128) k_glb_qt(Geom g, GlbJob job) {
             const int i0 = max(k0, w), i1 = min(k1, m - 1 - w);
             int k = k0;
             for (; k <= k1 && k < i0; ++k) qt = dadd(qt, qt_term(METRIC, Q[k], k, m, w, lf, uf, mu, sg, inv, rok, arg));
-#pragma unroll 4
+            for (; k + 1 <= i1; k += 2) {  // two points, four quotients, one range test
+                double z4[4];
+                zdiv_group(
+                    [&](int u) {
+                        const int kk = k + (u & 1);
+                        if (u < 2) { const double a0 = lf[kk - w], a1 = lf[kk]; return dsub((a1 < a0) ? a1 : a0, mu); }
+                        const double b0 = uf[kk - w], b1 = uf[kk];
+                        return dsub((b0 < b1) ? b1 : b0, mu);
+                    },
+                    sg, inv, rok, z4);
+                qt = dadd(qt, qt_term_norm(METRIC, Q[k], z4[0], z4[2], arg));
+                qt = dadd(qt, qt_term_norm(METRIC, Q[k + 1], z4[1], z4[3], arg));
+            }
             for (; k <= i1; ++k) {
                 const double a0 = lf[k - w], a1 = lf[k], b0 = uf[k - w], b1 = uf[k];
                 qt = dadd(qt, qt_term_env(METRIC, Q[k], (a1 < a0) ? a1 : a0, (b0 < b1) ? b1 : b0, mu, sg, inv, rok,
