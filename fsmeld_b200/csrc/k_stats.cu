@@ -10,9 +10,10 @@
 //
 // Memory: lanes of a warp walk 32 different segments in lock step.  The raw
 // stream is staged through shared memory in tiles of kTile points (32
-// coalesced 256-byte loads per tile and stream) and the outputs are staged
-// the same way, so global traffic is one read of the target (plus the
-// m-1 halo per segment) and one coalesced write of mu and sigma.
+// coalesced 256-byte loads per tile and stream, prefetched into registers a
+// tile ahead) and the outputs are staged the same way, so global traffic is
+// one read of the target (plus the m-1 halo per segment) and one coalesced
+// write of mu and sigma.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -38,23 +39,41 @@ __global__ void __launch_bounds__(32) k_mvmean(const double* __restrict__ target
 
     double s1 = 0.0, s2 = 0.0;
     int nonfinite = 0;
-    for (int k0 = 0; k0 < mk; k0 += kTile) {
+    // the next tile's raw points are loaded into registers while the current
+    // tile is processed: every load of a tile is in flight at once, behind
+    // the previous tile's work (row r = segment s0 + r, column = lane)
+    double pin[32], pout[32];
+    auto load_tile = [&](int k0) {
         const int cnt = min(kTile, mk - k0);
+#pragma unroll
         for (int r = 0; r < 32; ++r) {
             const long long sr = s0 + r;
+            double vi = 0.0, vo = 0.0;
             if (sr < g.S && lane < cnt) {
                 const double* tp = target + g.off(sr);
-                tin[r * kPitch + lane] = tp[k0 + lane];
+                vi = tp[k0 + lane];
                 const int ko = k0 + lane - m;
-                tout[r * kPitch + lane] = (ko >= 0) ? tp[ko] : 0.0;
+                if (ko >= 0) vo = tp[ko];
             }
+            pin[r] = vi;
+            pout[r] = vo;
+        }
+    };
+    load_tile(0);
+    for (int k0 = 0; k0 < mk; k0 += kTile) {
+        const int cnt = min(kTile, mk - k0);
+#pragma unroll
+        for (int r = 0; r < 32; ++r) {
+            tin[r * kPitch + lane] = pin[r];
+            tout[r * kPitch + lane] = pout[r];
         }
         __syncwarp();
+        if (k0 + kTile < mk) load_tile(k0 + kTile);
+        // the running sums, point by point (the serial part); each emitted
+        // window's sums and non-finite flag are staged for the second pass
         for (int x = 0; x < cnt; ++x) {
             const int k = k0 + x;
             const double incoming_raw = tin[lane * kPitch + x];
-            double mean = 0.0, sd = 0.0;
-            bool emit = false;
             if (k < m) {
                 // initial window (src/mvmean.cpp:16-27)
                 if (isfinite(incoming_raw)) {
@@ -63,7 +82,6 @@ __global__ void __launch_bounds__(32) k_mvmean(const double* __restrict__ target
                 } else {
                     ++nonfinite;
                 }
-                emit = (k == m - 1);
             } else {
                 // slide by one (src/mvmean.cpp:32-44)
                 const double outgoing_raw = tout[lane * kPitch + x];
@@ -73,11 +91,22 @@ __global__ void __launch_bounds__(32) k_mvmean(const double* __restrict__ target
                 nonfinite += (int)!inf - (int)!of;
                 s1 = dadd(dsub(s1, outgoing), incoming);
                 s2 = dadd(dsub(s2, dmul(outgoing, outgoing)), dmul(incoming, incoming));
-                emit = true;
             }
-            if (emit) {
-                mean = nonfinite ? qnan : ddiv(s1, dm);
-                sd = nonfinite ? qnan : dsqrt(dsub(ddiv(s2, dm), dmul(mean, mean)));
+            if (k >= m - 1) {  // a window ends here
+                smu[lane * kPitch + x] = s1;
+                ssg[lane * kPitch + x] = s2;
+                tin[lane * kPitch + x] = nonfinite ? 1.0 : 0.0;
+            }
+        }
+        // mean and sigma of every emitted window: independent of each other,
+        // so consecutive windows' divisions and square roots overlap
+#pragma unroll 4
+        for (int x = 0; x < cnt; ++x) {
+            if (k0 + x >= m - 1) {
+                const double a1 = smu[lane * kPitch + x], a2 = ssg[lane * kPitch + x];
+                const bool bad = tin[lane * kPitch + x] != 0.0;
+                const double mean = bad ? qnan : ddiv(a1, dm);
+                const double sd = bad ? qnan : dsqrt(dsub(ddiv(a2, dm), dmul(mean, mean)));
                 smu[lane * kPitch + x] = mean;
                 ssg[lane * kPitch + x] = sd;
             }
