@@ -370,7 +370,7 @@ static int run_stats(fsmeld_ctx* c, const Geom& g, Stats* st, const std::string&
     if ((r = allow_smem(c, k_mvmean, smem))) return r;
     const unsigned blocks = (unsigned)((g.S + 31) / 32);
     prof_begin(c, ST_STATS);
-    k_mvmean<<<blocks, 32, smem, c->stream>>>(c->d_target, g, st->MU, st->SIG);
+    k_mvmean<<<blocks, kMvmeanThreads, smem, c->stream>>>(c->d_target, g, st->MU, st->SIG);
     LAUNCH_CHECK(c);
     return FSMELD_OK;
 }

@@ -11,9 +11,14 @@
 // Memory: lanes of a warp walk 32 different segments in lock step.  The raw
 // stream is staged through shared memory in tiles of kTile points (32
 // coalesced 256-byte loads per tile and stream, prefetched into registers a
-// tile ahead) and the outputs are staged the same way, so global traffic is
-// one read of the target (plus the m-1 halo per segment) and one coalesced
-// write of mu and sigma.
+// tile ahead), so global traffic is one read of the target (plus the m-1 halo
+// per segment) and one coalesced write of mu and sigma.
+//
+// Work split: warp 0 of the block runs the 32 running-sum chains (the serial
+// part) and stages each emitted window's sums and non-finite flag in a
+// double-buffered tile; warps 1-3 turn the previous tile's sums into mean
+// and sigma (two divisions and a square root per window, independent of
+// each other) and write them out, so the chains never wait for them.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -22,27 +27,48 @@ namespace fsm {
 namespace {
 constexpr int kTile = 32;
 constexpr int kPitch = kTile + 1;  // padded rows: lane-strided smem reads hit distinct banks
+constexpr int kTileDoubles = 32 * kPitch;
 }
 
-__global__ void __launch_bounds__(32) k_mvmean(const double* __restrict__ target, Geom g,
-                                               double* __restrict__ mu, double* __restrict__ sig) {
+__global__ void __launch_bounds__(kMvmeanThreads) k_mvmean(const double* __restrict__ target, Geom g,
+                                                           double* __restrict__ mu, double* __restrict__ sig) {
     extern __shared__ double sm[];
-    double* tin = sm;                  // [32][kPitch] incoming points t[k]
-    double* tout = sm + 32 * kPitch;   // [32][kPitch] outgoing points t[k-m]
-    double* smu = sm + 64 * kPitch;    // [32][kPitch] staged means
-    double* ssg = sm + 96 * kPitch;    // [32][kPitch] staged sigmas
-    const int lane = threadIdx.x;
+    double* tin = sm;                        // [32][kPitch] incoming points t[k] (warp 0)
+    double* tout = sm + kTileDoubles;        // [32][kPitch] outgoing points t[k-m] (warp 0)
+    double* S1 = sm + 2 * kTileDoubles;      // [2][32][kPitch] staged sums, by tile parity
+    double* S2 = sm + 4 * kTileDoubles;      // [2][32][kPitch] staged sums of squares
+    int* FL = (int*)(sm + 6 * kTileDoubles); // [2][32][kPitch] staged non-finite flags
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
     const long long s0 = (long long)blockIdx.x * 32;
     const int m = g.m, mk = g.m_k, kml = g.kml;
-    const double dm = (double)m;
-    const double qnan = dnan();
+    const int ntiles = (mk + kTile - 1) / kTile;
 
+    // consumers (warps 1-3): mean and sigma of the emitted windows of tile t
+    auto finish_tile = [&](int t) {
+        const int k0 = t * kTile, cnt = min(kTile, mk - k0);
+        const int b = t & 1;
+        const double dm = (double)m;
+        const double qnan = dnan();
+        for (int idx = tid - 32; idx < 32 * kTile; idx += kMvmeanThreads - 32) {
+            const int r = idx / kTile, x = idx % kTile;  // segment s0 + r, point k0 + x
+            const long long sr = s0 + r;
+            if (x < cnt && k0 + x >= m - 1 && sr < g.S) {
+                const int o = b * kTileDoubles + r * kPitch + x;
+                const bool bad = FL[o] != 0;
+                const double mean = bad ? qnan : ddiv(S1[o], dm);
+                const double sd = bad ? qnan : dsqrt(dsub(ddiv(S2[o], dm), dmul(mean, mean)));
+                const long long w = sr * kml + (k0 + x - m + 1);
+                mu[w] = mean;
+                sig[w] = sd;
+            }
+        }
+    };
+
+    // producer (warp 0): the running sums of segment s0 + lane
     double s1 = 0.0, s2 = 0.0;
     int nonfinite = 0;
-    // the next tile's raw points are loaded into registers while the current
-    // tile is processed: every load of a tile is in flight at once, behind
-    // the previous tile's work (row r = segment s0 + r, column = lane)
-    double pin[32], pout[32];
+    double pin[32], pout[32];  // the next tile (row r = segment s0 + r, column = lane)
     auto load_tile = [&](int k0) {
         const int cnt = min(kTile, mk - k0);
 #pragma unroll
@@ -59,75 +85,58 @@ __global__ void __launch_bounds__(32) k_mvmean(const double* __restrict__ target
             pout[r] = vo;
         }
     };
-    load_tile(0);
-    for (int k0 = 0; k0 < mk; k0 += kTile) {
-        const int cnt = min(kTile, mk - k0);
+    if (tid < 32) load_tile(0);
+    for (int t = 0; t <= ntiles; ++t) {
+        if (tid < 32) {
+            if (t < ntiles) {
+                const int k0 = t * kTile, cnt = min(kTile, mk - k0);
+                const int b = t & 1;
 #pragma unroll
-        for (int r = 0; r < 32; ++r) {
-            tin[r * kPitch + lane] = pin[r];
-            tout[r * kPitch + lane] = pout[r];
-        }
-        __syncwarp();
-        if (k0 + kTile < mk) load_tile(k0 + kTile);
-        // the running sums, point by point (the serial part); each emitted
-        // window's sums and non-finite flag are staged for the second pass
-        for (int x = 0; x < cnt; ++x) {
-            const int k = k0 + x;
-            const double incoming_raw = tin[lane * kPitch + x];
-            if (k < m) {
-                // initial window (src/mvmean.cpp:16-27)
-                if (isfinite(incoming_raw)) {
-                    s1 = dadd(s1, incoming_raw);
-                    s2 = dadd(s2, dmul(incoming_raw, incoming_raw));
-                } else {
-                    ++nonfinite;
+                for (int r = 0; r < 32; ++r) {
+                    tin[r * kPitch + lane] = pin[r];
+                    tout[r * kPitch + lane] = pout[r];
                 }
-            } else {
-                // slide by one (src/mvmean.cpp:32-44)
-                const double outgoing_raw = tout[lane * kPitch + x];
-                const bool of = isfinite(outgoing_raw), inf = isfinite(incoming_raw);
-                const double outgoing = of ? outgoing_raw : 0.0;
-                const double incoming = inf ? incoming_raw : 0.0;
-                nonfinite += (int)!inf - (int)!of;
-                s1 = dadd(dsub(s1, outgoing), incoming);
-                s2 = dadd(dsub(s2, dmul(outgoing, outgoing)), dmul(incoming, incoming));
-            }
-            if (k >= m - 1) {  // a window ends here
-                smu[lane * kPitch + x] = s1;
-                ssg[lane * kPitch + x] = s2;
-                tin[lane * kPitch + x] = nonfinite ? 1.0 : 0.0;
-            }
-        }
-        // mean and sigma of every emitted window: independent of each other,
-        // so consecutive windows' divisions and square roots overlap
-#pragma unroll 4
-        for (int x = 0; x < cnt; ++x) {
-            if (k0 + x >= m - 1) {
-                const double a1 = smu[lane * kPitch + x], a2 = ssg[lane * kPitch + x];
-                const bool bad = tin[lane * kPitch + x] != 0.0;
-                const double mean = bad ? qnan : ddiv(a1, dm);
-                const double sd = bad ? qnan : dsqrt(dsub(ddiv(a2, dm), dmul(mean, mean)));
-                smu[lane * kPitch + x] = mean;
-                ssg[lane * kPitch + x] = sd;
-            }
-        }
-        __syncwarp();
-        // events x >= xs of this tile emitted windows k0 + x - m + 1
-        const int xs = max(0, m - 1 - k0);
-        if (xs < cnt) {
-            for (int r = 0; r < 32; ++r) {
-                const long long sr = s0 + r;
-                if (sr < g.S && lane >= xs && lane < cnt) {
-                    const long long o = sr * kml + (k0 + lane - m + 1);
-                    mu[o] = smu[r * kPitch + lane];
-                    sig[o] = ssg[r * kPitch + lane];
+                __syncwarp();
+                if (k0 + kTile < mk) load_tile(k0 + kTile);
+                for (int x = 0; x < cnt; ++x) {
+                    const int k = k0 + x;
+                    const double incoming_raw = tin[lane * kPitch + x];
+                    if (k < m) {
+                        // initial window (src/mvmean.cpp:16-27)
+                        if (isfinite(incoming_raw)) {
+                            s1 = dadd(s1, incoming_raw);
+                            s2 = dadd(s2, dmul(incoming_raw, incoming_raw));
+                        } else {
+                            ++nonfinite;
+                        }
+                    } else {
+                        // slide by one (src/mvmean.cpp:32-44)
+                        const double outgoing_raw = tout[lane * kPitch + x];
+                        const bool of = isfinite(outgoing_raw), inf = isfinite(incoming_raw);
+                        const double outgoing = of ? outgoing_raw : 0.0;
+                        const double incoming = inf ? incoming_raw : 0.0;
+                        nonfinite += (int)!inf - (int)!of;
+                        s1 = dadd(dsub(s1, outgoing), incoming);
+                        s2 = dadd(dsub(s2, dmul(outgoing, outgoing)), dmul(incoming, incoming));
+                    }
+                    if (k >= m - 1) {  // a window ends here
+                        const int o = b * kTileDoubles + lane * kPitch + x;
+                        S1[o] = s1;
+                        S2[o] = s2;
+                        FL[o] = nonfinite;
+                    }
                 }
+                __syncwarp();
             }
+        } else if (t > 0) {
+            finish_tile(t - 1);
         }
-        __syncwarp();
+        // tile t is staged and tile t-1 consumed: the producer may overwrite
+        // buffer (t-1) & 1 with tile t+1
+        __syncthreads();
     }
 }
 
-size_t mvmean_smem_bytes() { return sizeof(double) * 4 * 32 * kPitch; }
+size_t mvmean_smem_bytes() { return sizeof(double) * 6 * kTileDoubles + sizeof(int) * 2 * kTileDoubles; }
 
 }  // namespace fsm

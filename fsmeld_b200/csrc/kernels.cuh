@@ -75,6 +75,9 @@ struct DpJob {
     const double* cutoff_ptr;   // when set: the cutoff in device memory (read at kernel start)
 };
 
+// window statistics: one block per 32 segments, warp 0 runs the running sums
+// and warps 1-3 derive mean and sigma
+constexpr int kMvmeanThreads = 128;
 __global__ void k_mvmean(const double* __restrict__ target, Geom g, double* __restrict__ mu,
                          double* __restrict__ sig);
 template <int T, int OPT, bool GW>

@@ -197,7 +197,7 @@ extern "C" int fsmeld_exact_noalloc(int device, const double* device_target, int
     const size_t sm_stats = mvmean_smem_bytes();
     if ((e = raise_smem_limit((const void*)k_mvmean, device, sm_stats)) != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute", __FILE__, __LINE__);
-    k_mvmean<<<(unsigned)((g.S + 31) / 32), 32, sm_stats, st>>>(device_target, g, MU, SIG);
+    k_mvmean<<<(unsigned)((g.S + 31) / 32), kMvmeanThreads, sm_stats, st>>>(device_target, g, MU, SIG);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "k_mvmean", __FILE__, __LINE__);
 
     QueryDev qd{};
