@@ -50,6 +50,13 @@ struct MMComb {
     }
 };
 
+// Padded index of the per-segment arrays: one spare slot after every 8
+// elements, so the blocked walks of the scans (thread t on elements
+// [8t, 8t+8)) fall on distinct banks.
+__device__ __forceinline__ int px(int i) { return i + (i >> 3); }
+// slots for indices 0..n (the NaN prefix count reads index n)
+__host__ __device__ inline int env_pad_len(int n) { return n + (n >> 3) + 2; }
+
 template <int T>
 struct EnvTemp {
     union {
@@ -70,7 +77,7 @@ __device__ void seg_scan(double* mn, double* mx, int n, int B, EnvTemp<T>& tmp) 
     for (int u = lo; u < hi; ++u) {
         const int i = REV ? n - 1 - u : u;
         const bool start = REV ? (u == 0 || (i % B) == B - 1) : ((i % B) == 0);
-        const double xmn = mn[i], xmx = mx[i];
+        const double xmn = mn[px(i)], xmx = mx[px(i)];
         if (start || !(fl & 2)) {
             rmn = xmn;
             rmx = xmx;
@@ -83,8 +90,8 @@ __device__ void seg_scan(double* mn, double* mx, int n, int B, EnvTemp<T>& tmp) 
             rmn = (rmn <= xmn) ? rmn : xmn;
             rmx = (rmx >= xmx) ? rmx : xmx;
         }
-        mn[i] = rmn;
-        mx[i] = rmx;
+        mn[px(i)] = rmn;
+        mx[px(i)] = rmx;
     }
     MMCarry mine{rmn, rmx, fl}, cin;
     cub::BlockScan<MMCarry, T>(tmp.mm).ExclusiveScan(mine, cin, MMComb<REV>());
@@ -94,11 +101,11 @@ __device__ void seg_scan(double* mn, double* mx, int n, int B, EnvTemp<T>& tmp) 
         for (int u = lo; u < e; ++u) {
             const int i = REV ? n - 1 - u : u;
             if (!REV) {
-                mn[i] = (mn[i] <= cin.mn) ? mn[i] : cin.mn;
-                mx[i] = (mx[i] >= cin.mx) ? mx[i] : cin.mx;
+                mn[px(i)] = (mn[px(i)] <= cin.mn) ? mn[px(i)] : cin.mn;
+                mx[px(i)] = (mx[px(i)] >= cin.mx) ? mx[px(i)] : cin.mx;
             } else {
-                mn[i] = (cin.mn <= mn[i]) ? cin.mn : mn[i];
-                mx[i] = (cin.mx >= mx[i]) ? cin.mx : mx[i];
+                mn[px(i)] = (cin.mn <= mn[px(i)]) ? cin.mn : mn[px(i)];
+                mx[px(i)] = (cin.mx >= mx[px(i)]) ? cin.mx : mx[px(i)];
             }
         }
     }
@@ -121,8 +128,8 @@ __device__ void minmax_phase(const double* __restrict__ src, int n, int par, int
     int local_nan = 0;
     for (int i = t; i < n; i += T) {
         const double v = src[i];
-        wk.raw[i] = v;
-        wk.Pmn[i] = v; wk.Pmx[i] = v; wk.Smn[i] = v; wk.Smx[i] = v;
+        wk.raw[px(i)] = v;
+        wk.Pmn[px(i)] = v; wk.Pmx[px(i)] = v; wk.Smn[px(i)] = v; wk.Smx[px(i)] = v;
         local_nan |= isnan(v) ? 1 : 0;
     }
     const int any_nan = __syncthreads_or(local_nan);
@@ -130,14 +137,14 @@ __device__ void minmax_phase(const double* __restrict__ src, int n, int par, int
         const int c = (n + T - 1) / T;
         const int lo = t * c, hi = min(n, lo + c);
         int cnt = 0;
-        for (int i = lo; i < hi; ++i) cnt += isnan(wk.raw[i]) ? 1 : 0;
+        for (int i = lo; i < hi; ++i) cnt += isnan(wk.raw[px(i)]) ? 1 : 0;
         int off;
         cub::BlockScan<int, T>(tmp.ic).ExclusiveSum(cnt, off);
         for (int i = lo; i < hi; ++i) {
-            wk.ncnt[i] = off;
-            off += isnan(wk.raw[i]) ? 1 : 0;
+            wk.ncnt[px(i)] = off;
+            off += isnan(wk.raw[px(i)]) ? 1 : 0;
         }
-        if (hi == n && lo < hi) wk.ncnt[n] = off;  // the chunk holding n-1 closes the count
+        if (hi == n && lo < hi) wk.ncnt[px(n)] = off;  // the chunk holding n-1 closes the count
     }
     __syncthreads();
     seg_scan<T, false>(wk.Pmn, wk.Pmx, n, B, tmp);
@@ -150,29 +157,29 @@ __device__ void minmax_phase(const double* __restrict__ src, int n, int par, int
             int ws, we;
             if (CENTRED) { ws = max(0, o - par); we = min(n - 1, o + par); }
             else { ws = max(0, o - par + 1); we = min(o, n - 1); }
-            const bool nanwin = any_nan && (wk.ncnt[we + 1] - wk.ncnt[ws] > 0);
+            const bool nanwin = any_nan && (wk.ncnt[px(we + 1)] - wk.ncnt[px(ws)] > 0);
             if (nanwin) {
-                double a = wk.raw[ws];
+                double a = wk.raw[px(ws)];
                 if (isnan(a)) {
                     vmn = a; vmx = a;
                 } else {
                     vmn = a; vmx = a;
                     for (int i = ws + 1; i <= we; ++i) {
-                        const double v = wk.raw[i];
+                        const double v = wk.raw[px(i)];
                         if (isnan(v)) break;
                         vmn = (v <= vmn) ? v : vmn;
                         vmx = (v >= vmx) ? v : vmx;
                     }
                 }
             } else if (ws % B == 0) {
-                vmn = wk.Pmn[we]; vmx = wk.Pmx[we];
+                vmn = wk.Pmn[px(we)]; vmx = wk.Pmx[px(we)];
             } else if (ws / B == we / B) {
-                vmn = wk.Smn[ws]; vmx = wk.Smx[ws];
+                vmn = wk.Smn[px(ws)]; vmx = wk.Smx[px(ws)];
             } else {
-                const double pm = wk.Pmn[we], sm = wk.Smn[ws];
-                const double px = wk.Pmx[we], sx = wk.Smx[ws];
+                const double pm = wk.Pmn[px(we)], sm = wk.Smn[px(ws)];
+                const double pxv = wk.Pmx[px(we)], sx = wk.Smx[px(ws)];
                 vmn = (pm <= sm) ? pm : sm;
-                vmx = (px >= sx) ? px : sx;
+                vmx = (pxv >= sx) ? pxv : sx;
             }
         }
         omn[k] = vmn;
@@ -194,12 +201,13 @@ __global__ void __launch_bounds__(T) k_envelope(const double* __restrict__ targe
     const int mk = g.m_k, kml = g.kml, m = g.m;
     double* base = GW ? gwork + (long long)blockIdx.x * slot_stride : (double*)env_smem;
     EnvWork wk;
+    const int pk = env_pad_len(mk);  // padded length of each array
     wk.raw = base;
-    wk.Pmn = base + mk;
-    wk.Pmx = base + 2 * mk;
-    wk.Smn = base + 3 * mk;
-    wk.Smx = base + 4 * mk;
-    wk.ncnt = (int*)(base + 5 * mk);
+    wk.Pmn = base + pk;
+    wk.Pmx = base + 2 * pk;
+    wk.Smn = base + 3 * pk;
+    wk.Smx = base + 4 * pk;
+    wk.ncnt = (int*)(base + 5 * pk);
     for (long long s = blockIdx.x; s < g.S; s += gridDim.x) {
         double simn[OPT], simx[OPT], mumn[OPT], mumx[OPT], lmn[OPT], lmx[OPT];
         minmax_phase<T, OPT, false>(SIG + s * kml, kml, m, mk, wk, tmp, simn, simx);
@@ -220,7 +228,7 @@ __global__ void __launch_bounds__(T) k_envelope(const double* __restrict__ targe
     }
 }
 
-size_t envelope_work_bytes(int m_k) { return (size_t)m_k * (5 * sizeof(double) + sizeof(int)) + 16; }
+size_t envelope_work_bytes(int m_k) { return (size_t)env_pad_len(m_k) * (5 * sizeof(double) + sizeof(int)) + 16; }
 
 #define FSM_ENV_INST(T, OPT)                                                                          \
     template __global__ void k_envelope<T, OPT, false>(const double*, const double*, const double*,  \
