@@ -46,6 +46,7 @@ CUTOFFS = {"dtw": 2.80906383446946, "erp": 5.138604886191949, "edr": 48.0, "lcss
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "roofline_traffic.json")
 LATENCY_REPS = 10  # plain single-query requests per query for the latency figures
+DEFAULT_CONCURRENCY = 4  # the library's default (fsmeld_set_concurrency)
 
 
 def log(*a):
@@ -336,6 +337,8 @@ def impl_ours(args):
     target, queries = make_workload(rank, args.n_points)
     geom = geometry(len(target), M)
     eng = api.Engine(target, device=local)
+    conc = args.concurrency or DEFAULT_CONCURRENCY
+    eng.set_concurrency(conc)
     metrics = [(mt, ag) for mt, ag in METRICS if args.case in (None, mt)]
     if args.case or args.fixed_cutoffs or args.n_points != N_POINTS:
         cutoffs = dict(CUTOFFS)  # profiling cases: the workload's constants, no setup launches
@@ -383,7 +386,7 @@ def impl_ours(args):
             cells[mt] += r["counters"]["dp_cells"]
     stages = eng.stage_times()
     eng.set_profiling(False)
-    eng.set_concurrency(4)
+    eng.set_concurrency(conc)
     t_local = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
     c_local = torch.tensor([float(cand)], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -687,6 +690,8 @@ def main():
                          "c5: serving loop with Poisson arrivals (latency)")
     ap.add_argument("--rate", type=float, default=50.0, help="c5: request arrivals per second")
     ap.add_argument("--queries", type=int, default=32, help="c4: number of queries")
+    ap.add_argument("--concurrency", type=int, default=None,
+                    help="queries of the batch running at once on worker streams (default: the library's)")
     ap.add_argument("--fixed-cutoffs", action="store_true",
                     help="use the workload's cutoff constants without recomputing them (profiling runs)")
     args = ap.parse_args()

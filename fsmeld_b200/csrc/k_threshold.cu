@@ -16,8 +16,10 @@
 //     which it fires (a binary search over the sorted values); ops are
 //     ordered by (step, stream, rank) -- the order the reference's loops
 //     perform them in;
-//  3. one thread replays the ops in that order, so m_p and C carry the
-//     reference's rounding bit for bit, and records the state after each op;
+//  3. the ops are replayed in that order, so m_p and C carry the reference's
+//     rounding bit for bit: lane j of warp 0 owns accumulator j (m_0..m_2, C)
+//     and adds each op's operand, pre-signed for it, recording the state
+//     after each op;
 //  4. every candidate reads its state, scores LB in parallel, and a block
 //     reduction takes the first maximum (NaN at index 0 wins, as in
 //     findMaxIndex, src/find_t_lp.cpp:206-216).
