@@ -305,40 +305,70 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
 
     unsigned long long valid_count = 0, cells = 0;
     bool drained = false;
+    // Work reservoir: the warp claims 32 consecutive work items with one
+    // atomic, lane j holds item rbase + j with its list entry, window
+    // statistics and cascade sum already loaded, and idle lanes take items
+    // rptr, rptr + 1, ... by shuffle.  The atomic's and the loads' latency is
+    // paid once per 32 refills instead of once per refill (a candidate ends
+    // every few rows under early abandon).  Every item is taken exactly once.
+    int rptr = 32;  // next unused reservoir item (32: empty)
+    long long r_gi = 0;
+    double r_mu = 0.0, r_sg = 1.0, r_S = 0.0;
+    int r_flags = 0;  // bit 0: a valid window, bit 1: its cascade sum is present
     for (;;) {
-        // refill idle lanes from the work counter (lanes that draw an invalid
+        // refill idle lanes from the reservoir (lanes that draw an invalid
         // window ask again)
         while (!drained) {
             const unsigned need = __ballot_sync(0xffffffffu, !active);
             if (!need) break;
-            const int leader = __ffs(need) - 1;
-            unsigned long long base = 0;
-            if (lane == leader) base = atomicAdd(job.next, (unsigned long long)__popc(need));
-            base = __shfl_sync(0xffffffffu, base, leader);
-            if (base >= n) { drained = true; break; }
-            bool fresh = false;
-            if (!active) {
-                const unsigned long long c = base + __popc(need & ((1u << lane) - 1));
+            if (rptr >= 32) {
+                unsigned long long base = 0;
+                if (lane == 0) base = atomicAdd(job.next, 32ull);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (base >= n) { drained = true; break; }
+                rptr = 0;
+                r_flags = 0;
+                const unsigned long long c = base + (unsigned long long)lane;
                 if (c < n) {
-                    gi = job.list ? job.list[c] : (long long)c;
+                    r_gi = job.list ? job.list[c] : (long long)c;
                     long long s;
                     int j;
-                    g.locate(gi, &s, &j);
-                    mu = job.MU[s * g.kml + j];
-                    sg = job.SIG[s * g.kml + j];
-                    if (!window_invalid(sg, g, gi)) {
-                        tp = job.target + gi;
-                        inv = ddiv(1.0, sg);
-                        rok = rcp_div_in_range(sg);
-                        if (job.lraw) { lr = job.lraw + gi; ur = job.uraw + gi; }
-                        ++valid_count;
-                        has_s = job.list_s && job.lraw && job.list_s[c] >= 0.0;
-                        Ssum = has_s ? job.list_s[c] : 0.0;
-                        exact = query_exact;
-                        fresh = true;
-                        active = true;
+                    g.locate(r_gi, &s, &j);
+                    r_mu = job.MU[s * g.kml + j];
+                    r_sg = job.SIG[s * g.kml + j];
+                    if (!window_invalid(r_sg, g, r_gi)) {
+                        r_flags = 1;
+                        if (job.list_s && job.lraw) {
+                            r_S = job.list_s[c];
+                            if (r_S >= 0.0) r_flags |= 2;
+                        }
                     }
                 }
+            }
+            const int rank = __popc(need & ((1u << lane) - 1));
+            const bool take = !active && rank < 32 - rptr;
+            const int src = take ? rptr + rank : lane;
+            const long long t_gi = __shfl_sync(0xffffffffu, r_gi, src);
+            const double t_mu = __shfl_sync(0xffffffffu, r_mu, src);
+            const double t_sg = __shfl_sync(0xffffffffu, r_sg, src);
+            const double t_S = __shfl_sync(0xffffffffu, r_S, src);
+            const int t_flags = __shfl_sync(0xffffffffu, r_flags, src);
+            rptr = min(32, rptr + __popc(need));
+            bool fresh = false;
+            if (take && (t_flags & 1)) {
+                gi = t_gi;
+                mu = t_mu;
+                sg = t_sg;
+                tp = job.target + gi;
+                inv = ddiv(1.0, sg);
+                rok = rcp_div_in_range(sg);
+                if (job.lraw) { lr = job.lraw + gi; ur = job.uraw + gi; }
+                ++valid_count;
+                has_s = (t_flags & 2) != 0;
+                Ssum = has_s ? t_S : 0.0;
+                exact = query_exact;
+                fresh = true;
+                active = true;
             }
             // The warp initialises each fresh lane's band, ring padding and
             // first w+1 candidate points together, one pass each, instead of
