@@ -38,11 +38,22 @@ M, W, K_TOP = 256, 13, 50
 METRICS = [("dtw", 0.0), ("erp", 0.0), ("edr", 0.25), ("lcss", 0.25), ("msm", 0.5)]
 WORKLOAD = ("five queries (dtw; erp g=0; edr eps=0.25; lcss eps=0.25; msm c=0.5), m=256, w=13, "
             "2^24-point float64 random walk + 200 motifs + NaN spans + flat runs; cutoff = k=50 exact distance")
-# k=50 exact distance of each query over the full rank-0 target (part of the
-# workload definition; the GPU arm re-derives them with its own `cutoff` and
-# records whether they agree, the CPU reference arm uses them as given).
-CUTOFFS = {"dtw": 2.80906383446946, "erp": 5.138604886191949, "edr": 48.0, "lcss": 0.265625,
-           "msm": 74.7957914893858}
+# k=50 exact distance of each query over the full rank-0 target: the
+# reference's own values, pinned by tests/golden/make_config_pins.py (the
+# reference's `search` finds at least 50 matches at each cutoff and fewer
+# than 50 just below it; tests/test_gpu_config_pins.py checks the GPU's top-50
+# rankings against the reference's).  The GPU arm re-derives them with its own
+# `cutoff` and records whether they agree; the CPU reference arm uses them.
+PINS_PATH = os.path.join(ROOT, "tests", "golden", "config_pins.json")
+
+
+def load_cutoffs():
+    with open(PINS_PATH) as f:
+        pins = json.load(f)["c2"]["metrics"]
+    return {mt: float.fromhex(pins[mt]["cutoff"]) for mt, _ in METRICS}
+
+
+CUTOFFS = load_cutoffs()
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "roofline_traffic.json")
 LATENCY_REPS = 10  # plain single-query requests per query for the latency figures
@@ -448,7 +459,8 @@ def impl_ours(args):
                        "n": args.n_points, "m": M, "w": W, "k": K_TOP,
                        "queries_per_step": len(metrics), "parallelism": f"{world} GPU(s), one target partition each",
                        "l2": "inputs larger than L2 (134 MB target per GPU)",
-                       "cutoffs": cutoffs, "cutoffs_match_workload_constants": cutoffs_match},
+                       "cutoffs": cutoffs, "cutoffs_source": "reference k=50 distances (tests/golden/config_pins.json)",
+                       "cutoffs_match_reference_pins": cutoffs_match},
             "queries_per_s": len(metrics) * world / (t_max_ms / 1e3 / args.steps),
             "roofline": roofline(stages, cells, peaks),
             "roofline_hbm": roofline_hbm(stages, geom, peaks),
@@ -526,6 +538,102 @@ def workload_c4(args):
                                    f"n={n} walk + bursts on 1% of points (N(0,5))", "n": n},
             "per_k": out, "rankings_checked_against_exact_scan": checked,
             "hbm_peak_gbs": peaks["hbm_gbs"]}
+    print(json.dumps(line))
+    return 0
+
+
+C3_METRICS = [("dtw", 0.0), ("erp", 0.0), ("edr", 0.25), ("lcss", 0.25), ("msm", 0.5)]
+C3_M_RANGE = (64, 1024)
+C3_K = 10
+
+
+def c3_queries(t, count, seed=303):
+    """count queries: m uniform on [64, 1024], metrics round-robin, w = floor(0.05 m)."""
+    from fsmeld_b200.synth import query_from
+    rng = np.random.default_rng(seed)
+    qs = []
+    for i in range(count):
+        m = int(rng.integers(C3_M_RANGE[0], C3_M_RANGE[1] + 1))
+        metric, arg = C3_METRICS[i % len(C3_METRICS)]
+        q, _ = query_from(t, m, rng)
+        qs.append(dict(query=q, m=m, metric=metric, w=(m * 5) // 100, arg=arg))
+    return qs
+
+
+def workload_c3(args):
+    """Batched mixed queries: 512 queries of uneven length (m uniform on
+    [64, 1024], metrics round-robin, w = floor(0.05 m)) over one 2^26-point
+    random walk, each at its own rank-10 exact distance.  queries/s of one
+    batched call (fsmeld_batch) against the plain form (one fsmeld_search per
+    query on the same resident target) and the plain drop-in command (one
+    `fsmeld search` process per query: file read, upload, search, print; a
+    sample of the queries).  The match sets of the batched and plain forms
+    must be identical."""
+    import torch
+
+    from fsmeld_b200 import api
+    from fsmeld_b200.synth import random_walk
+
+    n = args.n_points if args.n_points != N_POINTS else (1 << 26)
+    count = args.queries if args.queries != 32 else 512
+    t = random_walk(n, 3)
+    qs = c3_queries(t, count)
+    eng = api.Engine(t)
+    if args.concurrency:
+        eng.set_concurrency(args.concurrency)
+    t0 = time.perf_counter()
+    cres = eng.batch("cutoff", [dict(d, k=C3_K) for d in qs], capacity=C3_K)
+    for d, r in zip(qs, cres):
+        if r["status"] != 0:
+            raise RuntimeError(f"cutoff failed: {r['status']}")
+        d["cutoff"] = float(r["dist"][C3_K - 1])
+    setup_s = time.perf_counter() - t0
+    eng.batch("search", qs[:8])  # warm-up (workspace)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    bres = eng.batch("search", qs)
+    wall_b = time.perf_counter() - t0
+    dev_b = eng.last_call_ms
+    t0 = time.perf_counter()
+    pres = [eng.search(d["query"], d["m"], d["cutoff"], d["metric"], d["w"], d["arg"]) for d in qs]
+    wall_p = time.perf_counter() - t0
+    same = all(r["status"] == 0 and list(r["idx"]) == list(p[0]) for r, p in zip(bres, pres))
+    if not same:
+        raise RuntimeError("batched and plain match sets differ")
+    cand = sum(r["counters"]["valid"] for r in bres)
+    eng.close()
+    # the plain drop-in: one process per query, as the reference command runs
+    from fsmeld_b200.api import CLI_PATH
+    sample = qs[:args.dropin_sample]
+    dropin_s = None
+    if sample and os.path.exists(CLI_PATH):
+        with tempfile.TemporaryDirectory() as tmp:
+            tp = os.path.join(tmp, "target.bin")
+            t.astype("<f8").tofile(tp)
+            env = dict(os.environ, FSMELD_RESULTS_CSV=os.path.join(tmp, "r.csv"), FSMELD_QUIET_MATCHES="1")
+            t0 = time.perf_counter()
+            for i, d in enumerate(sample):
+                qp = os.path.join(tmp, f"q{i}.txt")
+                np.savetxt(qp, d["query"], fmt="%.17g")
+                subprocess.run([CLI_PATH, "search", tp, qp, str(d["m"]), repr(d["cutoff"]), d["metric"],
+                                str(d["w"]), repr(d["arg"])], env=env, stdout=subprocess.DEVNULL, check=True)
+            dropin_s = (time.perf_counter() - t0) / len(sample)
+    qps_b = count / wall_b
+    qps_p = count / wall_p
+    line = {"metric": "queries/s", "value": qps_b, "unit": "queries/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic (seeded random walk)",
+            "config": {"workload": f"c3: {count} queries, m uniform on [64, 1024], metrics round-robin "
+                                   f"(dtw, erp g=0, edr eps=0.25, lcss eps=0.25, msm c=0.5), w=floor(0.05 m), "
+                                   f"cutoff = rank-{C3_K} exact distance, n={n} random walk",
+                       "n": n, "queries": count, "distinct_m": len({d["m"] for d in qs}),
+                       "concurrency": args.concurrency or DEFAULT_CONCURRENCY},
+            "batched": {"queries_per_s": qps_b, "wall_s": wall_b, "device_ms": dev_b,
+                        "candidates_per_s": cand / wall_b},
+            "plain": {"queries_per_s": qps_p, "wall_s": wall_p},
+            "batched_speedup": qps_b / qps_p,
+            "plain_dropin": ({"queries_per_s": 1.0 / dropin_s, "sample": len(sample),
+                              "speedup_batched_vs_dropin": qps_b * dropin_s} if dropin_s else None),
+            "match_sets_identical": same, "cutoff_setup_s": setup_s}
     print(json.dumps(line))
     return 0
 
@@ -685,11 +793,14 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--case", choices=[m for m, _ in METRICS], help="one metric's query only (profiling runs)")
     ap.add_argument("--n-points", type=int, default=N_POINTS, help="target length (profiling runs)")
-    ap.add_argument("--workload", choices=["search5", "c4", "c5", "stream"], default="search5",
-                    help="c4: batched DTW top-k queries over a 2^27-point target (queries/s); "
+    ap.add_argument("--workload", choices=["search5", "c3", "c4", "c5", "stream"], default="search5",
+                    help="c3: 512 mixed queries, batched vs plain (queries/s); "
+                         "c4: batched DTW top-k queries over a 2^27-point target (queries/s); "
                          "c5: serving loop with Poisson arrivals (latency)")
     ap.add_argument("--rate", type=float, default=50.0, help="c5: request arrivals per second")
-    ap.add_argument("--queries", type=int, default=32, help="c4: number of queries")
+    ap.add_argument("--queries", type=int, default=32, help="c4: number of queries (c3: 512 unless given)")
+    ap.add_argument("--dropin-sample", type=int, default=8,
+                    help="c3: queries timed through the plain drop-in command, one process each")
     ap.add_argument("--concurrency", type=int, default=None,
                     help="queries of the batch running at once on worker streams (default: the library's)")
     ap.add_argument("--fixed-cutoffs", action="store_true",
@@ -697,6 +808,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return impl_reference(args)
+    if args.workload == "c3":
+        return workload_c3(args)
     if args.workload == "c4":
         return workload_c4(args)
     if args.workload == "c5":

@@ -81,6 +81,10 @@ def lib():
             "fsmeld_strerror": (C.c_char_p, [C.c_int]),
             "fsmeld_set_workspace_limit": (C.c_int, [ctxp, C.c_int64]),
             "fsmeld_set_concurrency": (C.c_int, [ctxp, C.c_int]),
+            "fsmeld_set_normalization": (C.c_int, [ctxp, C.c_int]),
+            "fsmeld_set_lb_form": (C.c_int, [ctxp, C.c_int]),
+            "fsmeld_set_tuning": (C.c_int, [ctxp, C.c_char_p]),
+            "fsmeld_normalization": (C.c_int, [ctxp]),
             "fsmeld_kernel_launches": (C.c_int64, [ctxp]),
             "fsmeld_set_profiling": (C.c_int, [ctxp, C.c_int]),
             "fsmeld_stage_times": (C.c_int, [ctxp, dp, ip, C.c_int]),
@@ -143,10 +147,16 @@ def _iptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_int64))
 
 
-class Engine:
-    """A target series resident on one GPU, queried through the C ABI."""
+TUNE_TABLE = os.path.join(_PKG, "tune_table.txt")
 
-    def __init__(self, target=None, *, path=None, device=0, device_ptr=None, n=None):
+
+class Engine:
+    """A target series resident on one GPU, queried through the C ABI.
+
+    tuning: the tuning table's text (see fsmeld_set_tuning); by default the
+    measured table fsmeld_b200/tune_table.txt when present; "" for none."""
+
+    def __init__(self, target=None, *, path=None, device=0, device_ptr=None, n=None, tuning=None):
         self._ctx = C.c_void_p()
         L = lib()
         if path is not None:
@@ -157,6 +167,15 @@ class Engine:
             t = np.ascontiguousarray(target, dtype=np.float64)
             _check(L.fsmeld_open(device, _dptr(t), len(t), C.byref(self._ctx)))
         self.n = L.fsmeld_target_length(self._ctx)
+        if tuning is None and os.path.exists(TUNE_TABLE):
+            with open(TUNE_TABLE) as f:
+                tuning = f.read()
+        if tuning:
+            self.set_tuning(tuning)
+
+    def set_tuning(self, table_text):
+        """Rules for the automatic kernel choices (fsmeld_set_tuning)."""
+        _check(lib().fsmeld_set_tuning(self._ctx, table_text.encode()), self._ctx)
 
     def load(self, target):
         """Replace the target (host array, e.g. pinned memory) keeping the workspace."""
@@ -205,6 +224,25 @@ class Engine:
     def set_concurrency(self, queries):
         """Queries of one (m, w) group of a batch run concurrently on this many streams."""
         _check(lib().fsmeld_set_concurrency(self._ctx, int(queries)), self._ctx)
+
+    def set_normalization(self, mode):
+        """'zscore' (default, the reference command line's mode) or 'raw'
+        (the reference's NormalizationMode::Raw, include/funcs.h:20-28)."""
+        if mode not in ("zscore", "raw"):
+            raise FsmeldError(E_ARG, f"unknown normalization mode: {mode}")
+        _check(lib().fsmeld_set_normalization(self._ctx, 1 if mode == "raw" else 0), self._ctx)
+
+    def set_lb_form(self, form):
+        """LB_IP form of batched searches of equal (m, w) and metric: 'auto',
+        'fft' (per query, the reference's) or 'gemm' (tensor-core product)."""
+        ids = {"auto": 0, "fft": 1, "gemm": 2}
+        if form not in ids:
+            raise FsmeldError(E_ARG, f"unknown LB_IP form: {form}")
+        _check(lib().fsmeld_set_lb_form(self._ctx, ids[form]), self._ctx)
+
+    @property
+    def normalization(self):
+        return "raw" if lib().fsmeld_normalization(self._ctx) == 1 else "zscore"
 
     def search(self, query, m, cutoff, metric, w, arg=0.0, exclude=(-1, -1), seg_counts=False):
         q = np.ascontiguousarray(query[:m], dtype=np.float64)

@@ -28,10 +28,30 @@ CLI = os.path.join(BINDIR, "fsmeld")
 
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+def _cutlass_include():
+    """CUTLASS / CuTe headers (header-only; the sm100 UMMA descriptor unions).
+    $FSMELD_CUTLASS_INCLUDE, else the copy vendored with flashinfer."""
+    env = os.environ.get("FSMELD_CUTLASS_INCLUDE")
+    if env:
+        return env
+    try:
+        import importlib.util
+        spec = importlib.util.find_spec("flashinfer")
+        if spec and spec.submodule_search_locations:
+            cand = os.path.join(list(spec.submodule_search_locations)[0], "data", "cutlass", "include")
+            if os.path.isdir(cand):
+                return cand
+    except Exception:
+        pass
+    raise RuntimeError("CUTLASS headers not found: set FSMELD_CUTLASS_INCLUDE")
+
+
+CUTLASS_INC = None
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-static-global-template-stub=false",
                   "-Xcompiler", "-fPIC,-ffp-contract=off", f"-I{INCLUDE}"]
 
-CU = ["k_stats", "k_envelope", "k_threshold", "k_lbip", "k_glb", "k_dp", "k_select", "engine", "noalloc"]
+CU = ["k_stats", "k_envelope", "k_threshold", "k_lbip", "k_glb", "k_dp", "k_dpw", "k_lbgemm", "k_select", "engine", "noalloc"]
 
 
 def _newer(src_files, out):
@@ -65,7 +85,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         obj = os.path.join(OBJ, name + ".o")
         objs.append(obj)
         if force or _newer([src] + hdrs, obj):
-            jobs.append([NVCC] + NVFLAGS + ["-c", src, "-o", obj])
+            extra = [f"-I{_cutlass_include()}"] if name == "k_lbgemm" else []
+            jobs.append([NVCC] + NVFLAGS + extra + ["-c", src, "-o", obj])
     drv_src = os.path.join(HOST, "cli_driver.cpp")
     drv_obj = os.path.join(OBJ, "cli_driver.o")
     objs.append(drv_obj)

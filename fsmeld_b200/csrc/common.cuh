@@ -65,6 +65,9 @@ struct Geom {
     long long tsn;         // n - m + 1 windows
     long long excl_b, excl_e;
     double inv_kml;        // fl(1 / kml), for the quotient estimate in locate()
+    // raw (non-normalised) mode: every window whose points are all finite gets
+    // mean 0 and sigma 1, so the z-normalisation (t - 0) / 1 leaves it as is
+    int raw = 0;
     __host__ __device__ long long off(long long s) const { return s < forsize ? s * kml : n - m_k; }
     __host__ __device__ int lo(long long s) const { return s < forsize ? 0 : tail_lo; }
     __host__ __device__ long long gidx(long long s, int j) const { return s * kml + (j - lo(s)); }

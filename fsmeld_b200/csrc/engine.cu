@@ -15,6 +15,7 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -115,7 +116,7 @@ static double fn_tl(double q, double C, int metric) {
     return q;
 }
 
-int prepare_query(const double* q, int m, int metric, int w, double arg, HostQuery* hq) {
+int prepare_query(const double* q, int m, int metric, int w, double arg, HostQuery* hq, bool raw) {
     if (m < 2) return fail(FSMELD_E_ARG, "m must be at least 2.");
     if (w < 0 || w >= m) return fail(FSMELD_E_ARG, "w must satisfy 0 <= w < m.");
     if (metric < DTW || metric > MSM) return fail(FSMELD_E_ARG, "Unsupported metric.");
@@ -131,12 +132,12 @@ int prepare_query(const double* q, int m, int metric, int w, double arg, HostQue
     const double mean = ex / m;
     double sd = ex2 / m;
     sd = std::sqrt(sd - mean * mean);
-    if (!std::isfinite(sd) || sd <= 1e-12)
+    if (!raw && (!std::isfinite(sd) || sd <= 1e-12))
         return fail(FSMELD_E_ARG,
                     "Query cannot be z-normalized: non-finite or near-zero standard deviation.");
     hq->m = m; hq->w = w; hq->metric = metric; hq->arg = arg; hq->p = metric_p(metric);
     hq->qn.resize(m);
-    for (int i = 0; i < m; ++i) hq->qn[i] = (q[i] - mean) / sd;
+    for (int i = 0; i < m; ++i) hq->qn[i] = raw ? q[i] : (q[i] - mean) / sd;
     const std::vector<double>& qn = hq->qn;
     // query envelope (src/fsmeld.cpp:721): window extremes, most recent on ties
     hq->LQ.resize(m); hq->UQ.resize(m);
@@ -206,6 +207,21 @@ struct fsmeld_ctx {
     // FSMELD_DP_EXACT=1: run every DP candidate in the exact boundary mode
     // (same results; a diagnostic switch for the mode that in-range data never needs)
     bool dp_exact = false;
+    // FSMELD_DP_FORM: which exact-DP kernel runs -- 0 auto (the lane-per-candidate
+    // DP while its band and ring fit shared memory, else the wavefront), 1 the
+    // lane DP only (global band scratch for wide bands), 2 the wavefront
+    // wherever it applies (w <= 255).  Same results; a switch for tests and
+    // measurements.
+    int dp_form = 0;
+    // LB_IP form for batched searches of equal (m, w) and metric: 0 auto (the
+    // tuner's choice), 1 the per-query FFT form, 2 the tensor-core product
+    int lb_form = 0;
+    // tuning table (fsmeld_set_tuning): rules for the automatic choices
+    struct TuneRule { int kind, metric, m_k, lim, choice; };  // kind 0 dp, 1 lb
+    std::vector<TuneRule> tune;
+    // normalisation mode (the reference's set_normalization_mode, include/funcs.h:20-28):
+    // false z-score (the reference CLI's only mode), true raw
+    bool raw = false;
     double last_ms = 0.0;
     std::string err;
     struct Buf { void* p = nullptr; size_t bytes = 0; };
@@ -582,6 +598,18 @@ static int run_glb(fsmeld_ctx* c, const Geom& g, const QueryDev& qd, const Stats
     return FSMELD_OK;
 }
 
+// The tuning table's choice for a shape: the first rule of `kind` for the
+// metric and macro-segment length whose limit is >= v (dp: v = w, choice
+// 1 lane / 2 wave; lb: v = the group's query count as a lower limit, choice
+// 1 fft / 2 gemm).  0 when no rule matches.
+static int tuned(const fsmeld_ctx* c, int kind, int metric, int m_k, int v) {
+    for (const auto& t : c->tune) {
+        if (t.kind != kind || t.metric != metric || t.m_k != m_k) continue;
+        if (kind == 0 ? v <= t.lim : v >= t.lim) return t.choice;
+    }
+    return 0;
+}
+
 static int run_dp(fsmeld_ctx* c, const Geom& g, DpJob job, long long expected) {
     const int w = job.q.w;
     const int warps = kDpThreads / 32;
@@ -596,6 +624,25 @@ static int run_dp(fsmeld_ctx* c, const Geom& g, DpJob job, long long expected) {
     job.force_exact = c->dp_exact ? 1 : 0;
     unsigned grid;
     const bool gw_path = smem > (size_t)c->smem_optin - 4096;
+    // wide bands (and FSMELD_DP_FORM=wave): one warp per candidate, band in registers
+    int form = c->dp_form;
+    if (form == 0) form = tuned(c, 0, job.q.metric, g.m_k, w);
+    const void* wk = form == 1 ? nullptr : dpw_kernel(job.q.metric, w);
+    const size_t wsm = dpw_smem_bytes(job.q.m, kDpwThreads / 32);
+    if (wk && wsm + 1024 <= (size_t)c->smem_optin && (form == 2 || gw_path)) {
+        if ((r = allow_smem(c, wk, wsm))) return r;
+        int per_sm = 0;
+        FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wk, kDpwThreads, wsm));
+        const long long want = (expected + kDpwThreads / 32 - 1) / (kDpwThreads / 32);
+        grid = (unsigned)std::max<long long>(1, std::min<long long>(want, (long long)std::max(1, per_sm) * c->sm_count));
+        prof_begin(c, ST_DP);
+        Geom ga = g;
+        void* args[] = {&ga, &job};
+        const cudaError_t le = cudaLaunchKernel(wk, dim3(grid), dim3(kDpwThreads), args, wsm, c->stream);
+        if (le != cudaSuccess) return cuda_fail(le, "k_dpw launch", __FILE__, __LINE__);
+        LAUNCH_CHECK(c);
+        return FSMELD_OK;
+    }
     if (gw_path) {
         // band scratch in global memory (L2-resident per warp): 16 warps per SM
         const long long want = (expected + warps * 32 - 1) / (warps * 32);
@@ -675,6 +722,53 @@ struct QueryRun {
     int64_t* seg_counts;
 };
 
+// The search after LB_IP: GLB on the survivor list `surv` (count at
+// cnt[C_SURV]), the exact DP, ordered matches and counters.
+static int search_tail(fsmeld_ctx* c, const Geom& g, const QueryDev& qd, const Stats& st, long long* surv,
+                       unsigned long long* cnt, long long cap, long long* segc, const QueryRun& qr) {
+    int r;
+    unsigned long long h[C_N] = {0};
+    fsmeld_counters out{};
+    out.m_k = g.m_k;
+    out.segments = g.forsize;
+    out.tail = g.tsn % g.kml;
+    long long* g2;
+    double* g2t;
+    if ((r = run_glb(c, g, qd, st, surv, cnt, cap, segc, &g2, &g2t))) return r;
+    long long* oi;
+    double* od;
+    if ((r = bufT(c, "outi", (size_t)cap, &oi))) return r;
+    if ((r = bufT(c, "outd", (size_t)cap, &od))) return r;
+    DpJob dj{};
+    dj.q = qd; dj.target = c->d_target; dj.MU = st.MU; dj.SIG = st.SIG;
+    dj.lraw = st.Lraw; dj.uraw = st.Uraw;
+    dj.list = g2; dj.list_s = g2t; dj.n_list = cnt + C_G2; dj.list_cap = cap; dj.mode = 0; dj.cutoff = qr.cutoff;
+    dj.out_idx = oi; dj.out_dist = od; dj.n_out = cnt + C_OUT; dj.n_cells = cnt + C_CELLS; dj.out_cap = cap; dj.n_valid = nullptr;
+    if ((r = run_dp(c, g, dj, (long long)c->sm_count * 16 * 128))) return r;
+    FSM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const long long nout = (long long)h[C_OUT];
+    if ((r = sort_pairs_i64(c, oi, nullptr, nout))) return r;
+    const long long ncopy = std::min<long long>(nout, qr.cap);
+    if (ncopy > 0)
+        FSM_CUDA_TRY(cudaMemcpyAsync(qr.out_idx, oi, sizeof(long long) * ncopy, cudaMemcpyDeviceToHost, c->stream));
+    if (qr.seg_counts && segc && g.forsize > 0)
+        FSM_CUDA_TRY(cudaMemcpyAsync(qr.seg_counts, segc, sizeof(long long) * 3 * g.forsize,
+                                     cudaMemcpyDeviceToHost, c->stream));
+    FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    out.valid = (long long)h[C_VALID];
+    out.invalid = g.tsn - out.valid;
+    out.after_lb = (long long)h[C_SURV];
+    out.after_glb = (long long)h[C_G2];
+    out.exact_evals = out.after_glb;
+    out.matches = nout;
+    out.dp_cells = (long long)h[C_CELLS];
+    out.threshold = qr.cutoff;
+    if (qr.out_count) *qr.out_count = nout;
+    if (qr.cnt) *qr.cnt = out;
+    return FSMELD_OK;
+}
+
 static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& st, bool have_env) {
     int r;
     Geom g = g0;
@@ -745,41 +839,7 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
         lj.zout = nullptr; lj.surv = surv; lj.surv_cap = cap; lj.nsurv = cnt + C_SURV;
         lj.nvalid = cnt + C_VALID; lj.segc = segc;
         if ((r = run_lbip(c, g, lj))) return r;
-        long long* g2;
-        double* g2t;
-        if ((r = run_glb(c, g, qd, st, surv, cnt, cap, segc, &g2, &g2t))) return r;
-        long long* oi;
-        double* od;
-        if ((r = bufT(c, "outi", (size_t)cap, &oi))) return r;
-        if ((r = bufT(c, "outd", (size_t)cap, &od))) return r;
-        DpJob dj{};
-        dj.q = qd; dj.target = c->d_target; dj.MU = st.MU; dj.SIG = st.SIG;
-        dj.lraw = st.Lraw; dj.uraw = st.Uraw;
-        dj.list = g2; dj.list_s = g2t; dj.n_list = cnt + C_G2; dj.list_cap = cap; dj.mode = 0; dj.cutoff = qr.cutoff;
-        dj.out_idx = oi; dj.out_dist = od; dj.n_out = cnt + C_OUT; dj.n_cells = cnt + C_CELLS; dj.out_cap = cap; dj.n_valid = nullptr;
-        if ((r = run_dp(c, g, dj, (long long)c->sm_count * 16 * 128))) return r;
-        FSM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
-        FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
-        const long long nout = (long long)h[C_OUT];
-        if ((r = sort_pairs_i64(c, oi, nullptr, nout))) return r;
-        const long long ncopy = std::min<long long>(nout, qr.cap);
-        if (ncopy > 0)
-            FSM_CUDA_TRY(cudaMemcpyAsync(qr.out_idx, oi, sizeof(long long) * ncopy, cudaMemcpyDeviceToHost, c->stream));
-        if (qr.seg_counts && g.forsize > 0)
-            FSM_CUDA_TRY(cudaMemcpyAsync(qr.seg_counts, segc, sizeof(long long) * 3 * g.forsize,
-                                         cudaMemcpyDeviceToHost, c->stream));
-        FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
-        out.valid = (long long)h[C_VALID];
-        out.invalid = g.tsn - out.valid;
-        out.after_lb = (long long)h[C_SURV];
-        out.after_glb = (long long)h[C_G2];
-        out.exact_evals = out.after_glb;
-        out.matches = nout;
-        out.dp_cells = (long long)h[C_CELLS];
-        out.threshold = qr.cutoff;
-        if (qr.out_count) *qr.out_count = nout;
-        if (qr.cnt) *qr.cnt = out;
-        return FSMELD_OK;
+        return search_tail(c, g, qd, st, surv, cnt, cap, segc, qr);
     }
 
     // cutoff (top-k)
@@ -876,6 +936,224 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
     return FSMELD_OK;
 }
 
+// ------------------------------------------------ tensor-core LB_IP (groups)
+
+// src/q_to_h.cpp:11-64 (lower) / 84-134 (upper), the penalties of k_lbip
+static double host_q_to_h(int metric, bool upper, double x, double t, double C) {
+    auto sq = [](double a, double b) { const double d = a - b; return d * d; };
+    if (!upper) {
+        switch (metric) {
+            case MSM: return (x < t) ? ((t - x < C) ? t - x : C) : 0.0;
+            case DTW: return (x < t) ? sq(t, x) : 0.0;
+            case ERP: return (x < t) ? ((sq(x, t) > sq(x, C)) ? sq(x, C) : sq(x, t)) : 0.0;
+            default: return (x < t - C) ? 1.0 : 0.0;
+        }
+    }
+    switch (metric) {
+        case MSM: return (x > t) ? ((x - t < C) ? x - t : C) : 0.0;
+        case DTW: return (x > t) ? sq(x, t) : 0.0;
+        case ERP: return (x > t) ? ((sq(x, t) > sq(x, C)) ? sq(x, C) : sq(x, t)) : 0.0;
+        default: return (x > t + C) ? 1.0 : 0.0;
+    }
+}
+
+// round a double to BF16 (through float); the split below measures the
+// residual exactly, so the rounding direction does not matter
+static uint16_t to_bf16(double v) {
+    const float f = (float)v;
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)(u >> 16);  // inf / nan: truncate
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+static double from_bf16(uint16_t b) {
+    const uint32_t u = (uint32_t)b << 16;
+    float f;
+    memcpy(&f, &u, 4);
+    return (double)f;
+}
+
+struct GemmChoice {
+    double t_l = 0.0, t_u = 0.0;
+    bool ok = false;
+};
+
+// The group's thresholds: the medians over the segments of the thresholds
+// the reference's selection (k_threshold) picks for the group's first query.
+static int gemm_thresholds(fsmeld_ctx* c, const Geom& g, const Stats& st, const HostQuery& rep, GemmChoice* out) {
+    QueryDev qd;
+    int r;
+    if ((r = upload_query(c, rep, "query", &qd))) return r;
+    double* thr;
+    if ((r = bufT(c, "thr", (size_t)2 * g.S, &thr))) return r;
+    std::vector<ThrJob> jobs(1);
+    jobs[0].q = qd; jobs[0].Un = st.Un; jobs[0].Ln = st.Ln; jobs[0].thr = thr;
+    if ((r = run_thr(c, g, jobs))) return r;
+    std::vector<double> h(2 * (size_t)g.S);
+    FSM_CUDA_TRY(cudaMemcpyAsync(h.data(), thr, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+    FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    std::vector<double> tl, tu;
+    for (long long s = 0; s < g.S; ++s) {
+        if (std::isfinite(h[2 * s])) tl.push_back(h[2 * s]);
+        if (std::isfinite(h[2 * s + 1])) tu.push_back(h[2 * s + 1]);
+    }
+    out->ok = !tl.empty() && !tu.empty();
+    if (!out->ok) return FSMELD_OK;
+    std::nth_element(tl.begin(), tl.begin() + tl.size() / 2, tl.end());
+    std::nth_element(tu.begin(), tu.begin() + tu.size() / 2, tu.end());
+    out->t_l = tl[tl.size() / 2];
+    out->t_u = tu[tu.size() / 2];
+    return FSMELD_OK;
+}
+
+// Search for queries of equal (m, w) and metric with LB_IP as one
+// tensor-core product per chunk of up to 128 queries (k_lbgemm), then GLB and
+// the exact DP per query as in run_query.  Match sets are those of the
+// per-query path (every bound is a lower bound); the LB_IP survivor counters
+// differ (one shared threshold pair instead of one per segment and query).
+static int run_search_gemm(fsmeld_ctx* c, const Geom& g0, Stats& st, const std::vector<const QueryRun*>& qs,
+                           std::vector<int>* qstatus, double* zout_dev = nullptr, double* diag = nullptr) {
+    int r;
+    const int m = qs[0]->hq->m, w = qs[0]->hq->w, metric = qs[0]->hq->metric;
+    GemmChoice th;
+    if ((r = gemm_thresholds(c, g0, st, *qs[0]->hq, &th))) return r;
+    if (!th.ok) return FSMELD_E_UNSUPPORTED;  // no finite threshold: the caller runs the per-query path
+    const int kchunks = (m + kLbGemmKChunk - 1) / kLbGemmKChunk;
+    const int kpad = kchunks * kLbGemmKChunk;
+    const long long cap = g0.tsn;
+    const long long words = (g0.tsn + 31) / 32 + 1;
+    for (size_t q0 = 0; q0 < qs.size(); q0 += 128) {
+        const int nq = (int)std::min<size_t>(128, qs.size() - q0);
+        const int NQ = nq <= 16 ? 16 : nq <= 32 ? 32 : nq <= 64 ? 64 : 128;
+        // B operand and margins
+        std::vector<uint16_t> B((size_t)kchunks * 6 * NQ * kLbGemmKChunk, 0);
+        std::vector<double> marg(2 * (size_t)nq), cut(nq);
+        std::vector<int> met(nq);
+        std::vector<long long> eb(nq), ee(nq);
+        const double nadd = 3.0 * kpad + 16.0;
+        for (int i = 0; i < nq; ++i) {
+            const QueryRun& qr = *qs[q0 + i];
+            const HostQuery& hq = *qr.hq;
+            for (int side = 0; side < 2; ++side) {
+                const double t = side ? th.t_u : th.t_l;
+                double S = 0.0, R = 0.0;
+                for (int k = 0; k < m; ++k) {
+                    const double hv = host_q_to_h(hq.metric, side == 1, hq.qn[k], t, hq.arg);
+                    const uint16_t b0 = to_bf16(hv);
+                    const double r1 = hv - from_bf16(b0);
+                    const uint16_t b1 = to_bf16(r1);
+                    const double r2 = r1 - from_bf16(b1);
+                    const uint16_t b2 = to_bf16(r2);
+                    const double r3 = r2 - from_bf16(b2);
+                    S += std::fabs(from_bf16(b0)) + std::fabs(from_bf16(b1)) + std::fabs(from_bf16(b2));
+                    R += std::fabs(r3);
+                    const int ch = k / kLbGemmKChunk, kk = k % kLbGemmKChunk, kg = kk / 8, e = kk % 8;
+                    const uint16_t bs[3] = {b0, b1, b2};
+                    for (int sp = 0; sp < 3; ++sp) {
+                        const size_t off = (size_t)ch * 6 * NQ * kLbGemmKChunk +   // chunk
+                                           (size_t)(side * 3 + sp) * NQ * kLbGemmKChunk +  // sub-operand
+                                           (size_t)kg * NQ * 8 + (size_t)(i / 8) * 64 + (size_t)(i % 8) * 8 + e;
+                        B[off] = bs[sp];
+                    }
+                }
+                // FP32 accumulation of nadd terms (truncating adds bound each error by
+                // 2^-23 of the running magnitude <= S), times 4 for safety, plus the
+                // split's residual and a relative 2^-40 for these host sums
+                marg[2 * i + side] = (R + 4.0 * nadd * std::ldexp(S, -23)) * (1.0 + std::ldexp(1.0, -40)) + 1e-300;
+            }
+            cut[i] = qr.cutoff;
+            met[i] = hq.metric;
+            const bool ex = qr.eb >= 0 && qr.ee > qr.eb;
+            eb[i] = ex ? qr.eb : -1;
+            ee[i] = ex ? qr.ee : -1;
+        }
+        // upload
+        uint16_t* dB;
+        double *dM, *dC;
+        int* dMet;
+        long long *dE;
+        unsigned* dbits;
+        unsigned long long* dcnt;
+        if ((r = bufT(c, "gemmB", B.size(), &dB))) return r;
+        if ((r = bufT(c, "gemmM", 2 * (size_t)nq, &dM))) return r;
+        if ((r = bufT(c, "gemmC", (size_t)nq, &dC))) return r;
+        if ((r = bufT(c, "gemmMet", (size_t)nq, &dMet))) return r;
+        if ((r = bufT(c, "gemmE", 2 * (size_t)nq, &dE))) return r;
+        if ((r = bufT(c, "gemmBits", (size_t)nq * words, &dbits))) return r;
+        if ((r = bufT(c, "gemmCnt", 2 * (size_t)nq + 2, &dcnt))) return r;
+        std::vector<double> ml(nq), mu_(nq);
+        for (int i = 0; i < nq; ++i) { ml[i] = marg[2 * i]; mu_[i] = marg[2 * i + 1]; }
+        std::vector<long long> ebe(2 * (size_t)nq);
+        for (int i = 0; i < nq; ++i) { ebe[i] = eb[i]; ebe[nq + i] = ee[i]; }
+        FSM_CUDA_TRY(cudaMemcpyAsync(dB, B.data(), B.size() * 2, cudaMemcpyHostToDevice, c->stream));
+        FSM_CUDA_TRY(cudaMemcpyAsync(dM, ml.data(), 8 * (size_t)nq, cudaMemcpyHostToDevice, c->stream));
+        FSM_CUDA_TRY(cudaMemcpyAsync(dM + nq, mu_.data(), 8 * (size_t)nq, cudaMemcpyHostToDevice, c->stream));
+        FSM_CUDA_TRY(cudaMemcpyAsync(dC, cut.data(), 8 * (size_t)nq, cudaMemcpyHostToDevice, c->stream));
+        FSM_CUDA_TRY(cudaMemcpyAsync(dMet, met.data(), 4 * (size_t)nq, cudaMemcpyHostToDevice, c->stream));
+        FSM_CUDA_TRY(cudaMemcpyAsync(dE, ebe.data(), 16 * (size_t)nq, cudaMemcpyHostToDevice, c->stream));
+        FSM_CUDA_TRY(cudaMemsetAsync(dbits, 0, 4 * (size_t)nq * words, c->stream));
+        FSM_CUDA_TRY(cudaMemsetAsync(dcnt, 0, 8 * (2 * (size_t)nq + 2), c->stream));
+        GemmJob gj{};
+        gj.Un = st.Un; gj.Ln = st.Ln; gj.SIG = st.SIG; gj.t_l = th.t_l; gj.t_u = th.t_u;
+        gj.B = (const uint4*)dB; gj.m = m; gj.nq = nq; gj.kchunks = kchunks;
+        gj.margin_l = dM; gj.margin_u = dM + nq; gj.metric = dMet; gj.cutoff = dC;
+        gj.excl_b = dE; gj.excl_e = dE + nq;
+        gj.zout = zout_dev; gj.zstride = g0.S * g0.kml;
+        gj.bits = dbits; gj.bit_words = words;
+        gj.nsurv = dcnt; gj.nvalid = dcnt + nq; gj.err = (unsigned*)(dcnt + 2 * nq);
+        const void* kf = lbgemm_kernel(NQ);
+        const size_t smem = lbgemm_smem_bytes(NQ, m);
+        if ((r = allow_smem(c, kf, smem))) return r;
+        int per_sm = 0;
+        FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf, kLbGemmThreads, smem));
+        const int cols = std::max(32, 2 * NQ);
+        per_sm = std::max(1, std::min(per_sm, 512 / cols));  // TMEM: 512 columns per SM
+        const long long items = g0.S * ((g0.kml + 127) / 128);
+        const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(items, (long long)per_sm * c->sm_count));
+        Geom ga = g0;
+        void* args[] = {&ga, &gj};
+        prof_begin(c, ST_LBIP);
+        const cudaError_t le = cudaLaunchKernel(kf, dim3(grid), dim3(kLbGemmThreads), args, smem, c->stream);
+        if (le != cudaSuccess) return cuda_fail(le, "k_lbgemm launch", __FILE__, __LINE__);
+        LAUNCH_CHECK(c);
+        std::vector<unsigned long long> hc(2 * (size_t)nq + 2);
+        FSM_CUDA_TRY(cudaMemcpyAsync(hc.data(), dcnt, 8 * hc.size(), cudaMemcpyDeviceToHost, c->stream));
+        FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        if (hc[2 * nq] & 0xffffffffull) return fail(FSMELD_E_CUDA, "k_lbgemm: a bounded wait for the tensor cores gave up");
+        if (zout_dev) {  // diagnostics: the bounds, thresholds and margins of the first query only
+            if (diag) { diag[0] = th.t_l; diag[1] = th.t_u; diag[2] = marg[0]; diag[3] = marg[1]; }
+            return FSMELD_OK;
+        }
+        // per query: survivor list from its bits, then GLB + DP
+        for (int i = 0; i < nq; ++i) {
+            const QueryRun& qr = *qs[q0 + i];
+            Geom g = g0;
+            g.excl_b = eb[i];
+            g.excl_e = ee[i];
+            QueryDev qd;
+            if ((r = upload_query(c, *qr.hq, "query", &qd))) return r;
+            qd.cutoff = qr.cutoff;
+            unsigned long long* cnt;
+            if ((r = bufT(c, "counters", C_N, &cnt))) return r;
+            FSM_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, c->stream));
+            FSM_CUDA_TRY(cudaMemcpyAsync(cnt + C_VALID, dcnt + nq + i, 8, cudaMemcpyDeviceToDevice, c->stream));
+            long long* surv;
+            if ((r = bufT(c, "surv", (size_t)cap, &surv))) return r;
+            prof_begin(c, ST_LBIP);
+            k_bits_to_list<<<(unsigned)std::min<long long>((words + 255) / 256, (long long)c->sm_count * 8), 256, 0,
+                             c->stream>>>(dbits + (size_t)i * words, words, surv, cap, cnt + C_SURV);
+            LAUNCH_CHECK(c);
+            const int q = search_tail(c, g, qd, st, surv, cnt, cap, nullptr, qr);
+            (*qstatus)[q0 + i] = q;
+            if (q == FSMELD_E_CUDA) return q;
+        }
+    }
+    (void)w;
+    (void)metric;
+    return FSMELD_OK;
+}
+
 // One call over many queries: statistics per distinct m, envelopes per distinct (m, w).
 // worker context i of c (created on first use): same device and target, its
 // own stream and grow-only buffers
@@ -886,6 +1164,9 @@ static int get_worker(fsmeld_ctx* c, int i, fsmeld_ctx** out) {
         w->sm_count = c->sm_count;
         w->smem_optin = c->smem_optin;
         w->dp_exact = c->dp_exact;
+        w->dp_form = c->dp_form;
+        w->raw = c->raw;
+        w->lb_form = c->lb_form;
         if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreate(&w->ev0) != cudaSuccess || cudaEventCreate(&w->ev1) != cudaSuccess) {
             delete w;
@@ -899,14 +1180,134 @@ static int get_worker(fsmeld_ctx* c, int i, fsmeld_ctx** out) {
     w->n = c->n;
     w->ws_limit = c->ws_limit;
     w->prof = c->prof;
+    w->raw = c->raw;
+    w->lb_form = c->lb_form;
+    w->tune = c->tune;
     *out = w;
     return FSMELD_OK;
 }
 
+
+// Searches of one (m, w) group (order[gi..gj)) through the tensor-core LB_IP
+// when it is selected: one product per metric with at least two searches.
+// Marks the queries it ran in `done`.
+static int group_gemm(fsmeld_ctx* c, const Geom& g, Stats& st, std::vector<QueryRun>& runs,
+                      const std::vector<size_t>& order, size_t gi, size_t gj, std::vector<int>* status,
+                      std::vector<char>* done) {
+    if (c->lb_form == 1) return FSMELD_OK;
+    for (int metric = DTW; metric <= MSM; ++metric) {
+        std::vector<const QueryRun*> qs;
+        std::vector<size_t> idx;
+        for (size_t k = gi; k < gj; ++k) {
+            const QueryRun& qr = runs[order[k]];
+            if (qr.mode == 0 && qr.hq->metric == metric) { qs.push_back(&qr); idx.push_back(k); }
+        }
+        if (qs.size() < 2) continue;
+        if (c->lb_form == 0 && tuned(c, 1, metric, g.m_k, (int)qs.size()) != 2) continue;
+        std::vector<int> qst(qs.size(), FSMELD_OK);
+        const int r = run_search_gemm(c, g, st, qs, &qst);
+        if (r == FSMELD_E_UNSUPPORTED) continue;  // no usable threshold: per-query path
+        for (size_t t = 0; t < idx.size(); ++t) {
+            (*status)[order[idx[t]]] = r ? r : qst[t];
+            (*done)[idx[t]] = 1;
+        }
+        if (r == FSMELD_E_CUDA) return r;
+    }
+    return FSMELD_OK;
+}
+
+// fold a worker's profile and launch counts into its parent context
+static void absorb_worker(fsmeld_ctx* c, fsmeld_ctx* wk) {
+    cudaStreamSynchronize(wk->stream);
+    prof_collect(wk);
+    for (int k = 0; k < ST_N; ++k) {
+        c->stage_ms[k] += wk->stage_ms[k];
+        c->stage_n[k] += wk->stage_n[k];
+        wk->stage_ms[k] = 0.0;
+        wk->stage_n[k] = 0;
+    }
+    c->launches += wk->launches;
+    wk->launches = 0;
+}
+
+// Batches of many distinct query lengths: every distinct m is a task (its
+// window statistics, then for each of its radii the envelopes, then the
+// queries of each (m, w) group one after another), and the tasks run
+// concurrently on the worker streams, each worker with its own statistics,
+// envelopes and query buffers over the shared target.  Independent pipelines
+// on several streams keep the GPU busy through the latency-bound phases of
+// each (the running-sum statistics, the threshold replay, DP tails).
+static int run_tasks_parallel(fsmeld_ctx* c, std::vector<QueryRun>& runs, const std::vector<size_t>& order,
+                              const std::vector<std::pair<size_t, size_t>>& tasks, std::vector<int>* status) {
+    const int conc = std::min<int>(std::max(1, c->concurrency), (int)tasks.size());
+    std::vector<fsmeld_ctx*> ws(conc);
+    int r;
+    for (int t = 0; t < conc; ++t)
+        if ((r = get_worker(c, t, &ws[t]))) return r;
+    std::atomic<size_t> next{0};
+    std::atomic<bool> cuda_dead{false};
+    std::vector<std::string> errs(conc);
+    std::vector<std::thread> th;
+    for (int t = 0; t < conc; ++t) {
+        th.emplace_back([&, t] {
+            cudaSetDevice(c->device);
+            fsmeld_ctx* wk = ws[t];
+            for (;;) {
+                const size_t ti = next.fetch_add(1);
+                if (ti >= tasks.size() || cuda_dead.load()) break;
+                const size_t lo = tasks[ti].first, hi = tasks[ti].second;
+                auto mark = [&](size_t a, size_t b, int code) {
+                    for (size_t k = a; k < b; ++k) (*status)[order[k]] = code;
+                    if (errs[t].empty()) errs[t] = g_last_error;
+                    if (code == FSMELD_E_CUDA) cuda_dead = true;
+                };
+                Geom g{};
+                Stats st;
+                int q = make_geom(c->n, runs[order[lo]].hq->m, -1, -1, &g);
+                g.raw = c->raw ? 1 : 0;
+                if (!q) q = run_stats(wk, g, &st, "");
+                if (q) { mark(lo, hi, q); continue; }
+                size_t gi = lo;
+                while (gi < hi) {
+                    const int w = runs[order[gi]].hq->w;
+                    size_t gj = gi + 1;
+                    while (gj < hi && runs[order[gj]].hq->w == w) ++gj;
+                    bool need_env = false;
+                    for (size_t k = gi; k < gj; ++k) need_env = need_env || runs[order[k]].mode != 2;
+                    if (need_env && (q = run_env(wk, g, w, &st, ""))) { mark(gi, gj, q); gi = gj; continue; }
+                    std::vector<char> done(hi, 0);
+                    if ((q = group_gemm(wk, g, st, runs, order, gi, gj, status, &done)) == FSMELD_E_CUDA) {
+                        mark(gi, gj, q);
+                        break;
+                    }
+                    for (size_t k = gi; k < gj; ++k) {
+                        if (done[k]) continue;
+                        q = run_query(wk, runs[order[k]], g, st, need_env);
+                        (*status)[order[k]] = q;
+                        if (q) mark(k, k + 1, q);
+                        if (q == FSMELD_E_CUDA) break;
+                    }
+                    if (cuda_dead.load()) break;
+                    gi = gj;
+                }
+            }
+        });
+    }
+    for (auto& x : th) x.join();
+    for (int t = 0; t < conc; ++t) absorb_worker(c, ws[t]);
+    int first_err = FSMELD_OK;
+    for (size_t k = 0; k < order.size() && !first_err; ++k) first_err = (*status)[order[k]];
+    if (first_err)
+        for (auto& e : errs) if (!e.empty()) { g_last_error = e; break; }
+    return first_err;
+}
+
 // One call over many queries: statistics per distinct m, envelopes per distinct
-// (m, w); the queries of one (m, w) group then run concurrently on worker
-// streams (each query's pipeline is independent; its last step waits for its
-// own stream, so the group is done on the device when its threads return).
+// (m, w).  Several distinct lengths: the lengths run concurrently on worker
+// streams (run_tasks_parallel).  One length: the queries of each (m, w) group
+// run concurrently on worker streams (each query's pipeline is independent;
+// its last step waits for its own stream, so the group is done on the device
+// when its threads return).
 int run_batch(fsmeld_ctx* c, std::vector<QueryRun>& runs, std::vector<int>* status) {
     status->assign(runs.size(), FSMELD_OK);
     std::vector<size_t> order(runs.size());
@@ -915,6 +1316,16 @@ int run_batch(fsmeld_ctx* c, std::vector<QueryRun>& runs, std::vector<int>* stat
         if (runs[a].hq->m != runs[b].hq->m) return runs[a].hq->m < runs[b].hq->m;
         return runs[a].hq->w < runs[b].hq->w;
     });
+    {
+        std::vector<std::pair<size_t, size_t>> tasks;  // [lo, hi) of order per distinct m
+        for (size_t i = 0; i < order.size();) {
+            size_t j = i + 1;
+            while (j < order.size() && runs[order[j]].hq->m == runs[order[i]].hq->m) ++j;
+            tasks.emplace_back(i, j);
+            i = j;
+        }
+        if (tasks.size() > 1 && c->concurrency > 1) return run_tasks_parallel(c, runs, order, tasks, status);
+    }
     if (!c->ev_ready) FSM_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_ready, cudaEventDisableTiming));
     int cur_m = -1, cur_w = -1;
     Stats st;
@@ -931,6 +1342,7 @@ int run_batch(fsmeld_ctx* c, std::vector<QueryRun>& runs, std::vector<int>* stat
             have_env = false;
             cur_w = -1;
             r = make_geom(c->n, m, -1, -1, &g);
+            g.raw = c->raw ? 1 : 0;
             if (!r) r = run_stats(c, g, &st, "");
             cur_m = r ? -1 : m;
         }
@@ -948,12 +1360,20 @@ int run_batch(fsmeld_ctx* c, std::vector<QueryRun>& runs, std::vector<int>* stat
             oi = oj;
             continue;
         }
-        const int nq = (int)(oj - oi);
-        const int conc = std::min(std::max(1, c->concurrency), nq);
+        // searches through the tensor-core LB_IP (when selected), then the rest
+        std::vector<char> done(oj, 0);
+        if ((r = group_gemm(c, g, st, runs, order, oi, oj, status, &done)) == FSMELD_E_CUDA) return r;
+        std::vector<size_t> rest;
+        for (size_t k = oi; k < oj; ++k)
+            if (!done[k]) rest.push_back(order[k]);
+        for (size_t k = oi; k < oj; ++k)
+            if (done[k] && (*status)[order[k]] && !first_err) first_err = (*status)[order[k]];
+        const int nq = (int)rest.size();
+        const int conc = std::min(std::max(1, c->concurrency), std::max(1, nq));
         if (conc <= 1) {
-            for (size_t k = oi; k < oj; ++k) {
-                const int q = run_query(c, runs[order[k]], g, st, have_env);
-                (*status)[order[k]] = q;
+            for (size_t k : rest) {
+                const int q = run_query(c, runs[k], g, st, have_env);
+                (*status)[k] = q;
                 if (q && !first_err) first_err = q;
                 if (q == FSMELD_E_CUDA) break;
             }
@@ -969,33 +1389,21 @@ int run_batch(fsmeld_ctx* c, std::vector<QueryRun>& runs, std::vector<int>* stat
                     cudaSetDevice(c->device);
                     fsmeld_ctx* wk = ws[t];
                     if (cudaStreamWaitEvent(wk->stream, c->ev_ready, 0) != cudaSuccess) {
-                        for (int k = t; k < nq; k += conc) (*status)[order[oi + k]] = FSMELD_E_CUDA;
+                        for (int k = t; k < nq; k += conc) (*status)[rest[k]] = FSMELD_E_CUDA;
                         return;
                     }
                     for (int k = t; k < nq; k += conc) {
-                        const int q = run_query(wk, runs[order[oi + k]], g, st, have_env);
-                        (*status)[order[oi + k]] = q;
+                        const int q = run_query(wk, runs[rest[k]], g, st, have_env);
+                        (*status)[rest[k]] = q;
                         if (q && errs[t].empty()) errs[t] = g_last_error;
                         if (q == FSMELD_E_CUDA) break;
                     }
                 });
             }
             for (auto& x : th) x.join();
-            for (int t = 0; t < conc; ++t) {
-                fsmeld_ctx* wk = ws[t];
-                // a query that failed part-way may have left kernels queued: the next
-                // group rewrites the shared statistics only after they are done
-                cudaStreamSynchronize(wk->stream);
-                prof_collect(wk);
-                for (int k = 0; k < 8; ++k) {
-                    c->stage_ms[k] += wk->stage_ms[k];
-                    c->stage_n[k] += wk->stage_n[k];
-                    wk->stage_ms[k] = 0.0;
-                    wk->stage_n[k] = 0;
-                }
-                c->launches += wk->launches;
-                wk->launches = 0;
-            }
+            // a query that failed part-way may have left kernels queued: the next
+            // group rewrites the shared statistics only after they are done
+            for (int t = 0; t < conc; ++t) absorb_worker(c, ws[t]);
             for (size_t k = oi; k < oj; ++k) {
                 const int q = (*status)[order[k]];
                 if (q && !first_err) {
@@ -1028,6 +1436,8 @@ static int open_common(int device, fsmeld_ctx** out) {
     c->sm_count = prop.multiProcessorCount;
     c->smem_optin = (int)prop.sharedMemPerBlockOptin;
     if (const char* ex = getenv("FSMELD_DP_EXACT")) c->dp_exact = ex[0] == '1';
+    if (const char* f = getenv("FSMELD_DP_FORM")) c->dp_form = !strcmp(f, "lane") ? 1 : !strcmp(f, "wave") ? 2 : 0;
+    if (const char* f = getenv("FSMELD_LB_FORM")) c->lb_form = !strcmp(f, "fft") ? 1 : !strcmp(f, "gemm") ? 2 : 0;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
         delete c;
@@ -1119,6 +1529,56 @@ int fsmeld_close(fsmeld_ctx* c) {
 
 int64_t fsmeld_target_length(const fsmeld_ctx* c) { return c ? c->n : 0; }
 
+int fsmeld_set_normalization(fsmeld_ctx* c, int mode) {
+    if (!c || (mode != FSMELD_NORM_ZSCORE && mode != FSMELD_NORM_RAW))
+        return fail(FSMELD_E_ARG, "normalization mode must be FSMELD_NORM_ZSCORE or FSMELD_NORM_RAW");
+    c->raw = mode == FSMELD_NORM_RAW;
+    return FSMELD_OK;
+}
+
+int fsmeld_normalization(const fsmeld_ctx* c) { return (c && c->raw) ? FSMELD_NORM_RAW : FSMELD_NORM_ZSCORE; }
+
+int fsmeld_set_tuning(fsmeld_ctx* c, const char* table) {
+    if (!c) return fail(FSMELD_E_ARG, "null context");
+    std::vector<fsmeld_ctx::TuneRule> rules;
+    const char* p = table ? table : "";
+    while (*p) {
+        const char* e = strchr(p, '\n');
+        std::string line(p, e ? (size_t)(e - p) : strlen(p));
+        p = e ? e + 1 : p + strlen(p);
+        const size_t hash = line.find('#');
+        if (hash != std::string::npos) line.resize(hash);
+        char kind[8], metric[8], choice[8];
+        int mk = 0, lim = 0;
+        if (sscanf(line.c_str(), "%7s %7s %d %d %7s", kind, metric, &mk, &lim, choice) != 5) {
+            bool blank = true;
+            for (char ch : line) blank = blank && (ch == ' ' || ch == '\t' || ch == '\r');
+            if (blank) continue;
+            return fail(FSMELD_E_ARG, "tuning table: a line is not 'kind metric m_k limit choice'");
+        }
+        fsmeld_ctx::TuneRule t{};
+        t.kind = !strcmp(kind, "dp") ? 0 : !strcmp(kind, "lb") ? 1 : -1;
+        t.metric = !strcmp(metric, "dtw") ? DTW : !strcmp(metric, "erp") ? ERP : !strcmp(metric, "edr") ? EDR
+                 : !strcmp(metric, "lcss") ? LCSS : !strcmp(metric, "msm") ? MSM : -1;
+        t.m_k = mk;
+        t.lim = lim;
+        t.choice = (!strcmp(choice, "lane") || !strcmp(choice, "fft")) ? 1
+                 : (!strcmp(choice, "wave") || !strcmp(choice, "gemm")) ? 2 : -1;
+        if (t.kind < 0 || t.metric < 0 || t.choice < 0)
+            return fail(FSMELD_E_ARG, "tuning table: unknown kind, metric or choice");
+        rules.push_back(t);
+    }
+    c->tune = rules;
+    return FSMELD_OK;
+}
+
+int fsmeld_set_lb_form(fsmeld_ctx* c, int form) {
+    if (!c || form < FSMELD_LB_AUTO || form > FSMELD_LB_GEMM)
+        return fail(FSMELD_E_ARG, "LB_IP form must be FSMELD_LB_AUTO, FSMELD_LB_FFT or FSMELD_LB_GEMM");
+    c->lb_form = form;
+    return FSMELD_OK;
+}
+
 int fsmeld_set_concurrency(fsmeld_ctx* c, int queries) {
     if (!c || queries < 1 || queries > 16) return fail(FSMELD_E_ARG, "concurrency must be in [1, 16]");
     c->concurrency = queries;
@@ -1187,7 +1647,7 @@ static int single(fsmeld_ctx* c, int mode, const double* query, int m, double cu
     }
     FSM_CUDA_TRY(cudaSetDevice(c->device));
     HostQuery hq;
-    int r = prepare_query(query, m, metric, w, arg, &hq);
+    int r = prepare_query(query, m, metric, w, arg, &hq, c->raw);
     if (r) return r;
     QueryRun qr{&hq, mode, cutoff, k, eb, ee, out_idx, out_dist, cap, out_count, counters, seg_counts};
     std::vector<QueryRun> runs{qr};
@@ -1233,7 +1693,7 @@ int fsmeld_batch(fsmeld_ctx* c, int mode, const fsmeld_query* qs, int nq, fsmeld
     std::vector<int> map;
     for (int i = 0; i < nq; ++i) {
         res[i].count = 0;
-        res[i].status = prepare_query(qs[i].query, qs[i].m, qs[i].metric, qs[i].w, qs[i].arg, &hqs[i]);
+        res[i].status = prepare_query(qs[i].query, qs[i].m, qs[i].metric, qs[i].w, qs[i].arg, &hqs[i], c->raw);
         if (res[i].status) continue;
         if (mode == 1 && (qs[i].k < 1 || (long long)qs[i].k > c->n - qs[i].m + 1)) { res[i].status = FSMELD_E_ARG; continue; }
         if (mode != 1 && !(std::isfinite(qs[i].cutoff) && qs[i].cutoff >= 0)) { res[i].status = FSMELD_E_ARG; continue; }
@@ -1264,13 +1724,14 @@ int fsmeld_batch(fsmeld_ctx* c, int mode, const fsmeld_query* qs, int nq, fsmeld
 
 int64_t fsmeld_inspect(fsmeld_ctx* c, const double* query, int m, int metric, int w, double arg, int what,
                        double* out, int64_t cap) {
-    if (!c || !query || what < 0 || what > 5) return fail(FSMELD_E_ARG, "invalid inspect request");
+    if (!c || !query || what < 0 || what > 7) return fail(FSMELD_E_ARG, "invalid inspect request");
     FSM_CUDA_TRY(cudaSetDevice(c->device));
     HostQuery hq;
-    int r = prepare_query(query, m, metric, w, arg, &hq);
+    int r = prepare_query(query, m, metric, w, arg, &hq, c->raw);
     if (r) return r;
     Geom g;
     if ((r = make_geom(c->n, m, -1, -1, &g))) return r;
+    g.raw = c->raw ? 1 : 0;
     Stats st;
     if ((r = run_stats(c, g, &st, ""))) return r;
     const double* src = nullptr;
@@ -1294,6 +1755,24 @@ int64_t fsmeld_inspect(fsmeld_ctx* c, const double* query, int m, int metric, in
             if (what == 4) {
                 src = thr;
                 count = 2 * g.S;
+            } else if (what >= 6) {
+                // the tensor-core LB_IP of this query alone (its thresholds' medians)
+                double* z;
+                if ((r = bufT(c, "zbuf", (size_t)g.S * g.kml, &z))) return r;
+                QueryRun qr{&hq, 0, 0.0, 0, -1, -1, nullptr, nullptr, 0, nullptr, nullptr, nullptr};
+                std::vector<const QueryRun*> qs{&qr};
+                std::vector<int> qst(1);
+                double diag[4] = {0, 0, 0, 0};
+                qr.cutoff = 1e300;
+                if ((r = run_search_gemm(c, g, st, qs, &qst, z, diag))) return r;
+                if (what == 6) {
+                    src = z;
+                    count = g.S * g.kml;
+                } else {
+                    const long long nd = std::min<long long>(4, cap);
+                    if (out && nd > 0) memcpy(out, diag, sizeof(double) * nd);
+                    return 4;
+                }
             } else {
                 unsigned long long* cnt;
                 if ((r = bufT(c, "counters", C_N, &cnt))) return r;

@@ -16,7 +16,8 @@ struct HostQuery {
     std::vector<int> ordA_l, ordB_l, ordA_u, ordB_u;
 };
 
-int prepare_query(const double* q, int m, int metric, int w, double arg, HostQuery* hq);
+// raw: the query is used as given (no z-normalisation; raw mode)
+int prepare_query(const double* q, int m, int metric, int w, double arg, HostQuery* hq, bool raw = false);
 int macro_length(int m, long long available);
 extern thread_local std::string g_last_error;
 

@@ -14,6 +14,10 @@
 // tile ahead), so global traffic is one read of the target (plus the m-1 halo
 // per segment) and one coalesced write of mu and sigma.
 //
+// Raw (non-normalised) mode (g.raw): a window is valid iff its points are all
+// finite, and its statistics are mean 0 and sigma 1, so every later stage
+// sees the raw values ((t - 0) / 1 = t exactly) with the same code.
+//
 // Work split: warp 0 of the block runs the 32 running-sum chains (the serial
 // part) and stages each emitted window's sums and non-finite flag in a
 // double-buffered tile; warps 1-3 turn the previous tile's sums into mean
@@ -56,8 +60,14 @@ __global__ void __launch_bounds__(kMvmeanThreads) k_mvmean(const double* __restr
             if (x < cnt && k0 + x >= m - 1 && sr < g.S) {
                 const int o = b * kTileDoubles + r * kPitch + x;
                 const bool bad = FL[o] != 0;
-                const double mean = bad ? qnan : ddiv(S1[o], dm);
-                const double sd = bad ? qnan : dsqrt(dsub(ddiv(S2[o], dm), dmul(mean, mean)));
+                double mean, sd;
+                if (g.raw) {  // raw mode: valid iff every point is finite
+                    mean = bad ? qnan : 0.0;
+                    sd = bad ? qnan : 1.0;
+                } else {
+                    mean = bad ? qnan : ddiv(S1[o], dm);
+                    sd = bad ? qnan : dsqrt(dsub(ddiv(S2[o], dm), dmul(mean, mean)));
+                }
                 const long long w = sr * kml + (k0 + x - m + 1);
                 mu[w] = mean;
                 sig[w] = sd;

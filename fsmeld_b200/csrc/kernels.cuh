@@ -75,6 +75,38 @@ struct DpJob {
     const double* cutoff_ptr;   // when set: the cutoff in device memory (read at kernel start)
 };
 
+// LB_IP of a group of queries of equal (m, w) with shared thresholds as one
+// tensor-core product (k_lbgemm); per-query arrays are indexed by query
+struct GemmJob {
+    const double* Un;           // [S][m_k]
+    const double* Ln;
+    const double* SIG;          // [S][kml]
+    double t_l, t_u;            // the group's thresholds
+    const uint4* B;             // BF16 penalty operand, per K chunk [side][split][NQ x 64] (operand layout)
+    int m, nq, kchunks;
+    const double* margin_l;     // rounding-error margins of the lower / upper inner products
+    const double* margin_u;
+    const int* metric;
+    const double* cutoff;
+    const long long* excl_b;    // exclusion interval per query (-1: none)
+    const long long* excl_e;
+    double* zout;               // optional: bound per window, [q][zstride]
+    long long zstride;
+    unsigned* bits;             // survivors per query: bit g of bits[q * bit_words ...] (zeroed by the caller)
+    long long bit_words;
+    unsigned long long* nsurv;  // [nq]
+    unsigned long long* nvalid; // [nq]
+    unsigned int* err;          // set when a bounded wait gave up
+};
+template <int NQ>
+__global__ void k_lbgemm(Geom g, GemmJob job);
+const void* lbgemm_kernel(int nq_pad);  // NQ in {16, 32, 64, 128}
+__global__ void k_bits_to_list(const unsigned* __restrict__ bits, long long words, long long* __restrict__ out,
+                               long long cap, unsigned long long* __restrict__ n);
+size_t lbgemm_smem_bytes(int nq_pad, int m);
+constexpr int kLbGemmThreads = 128;
+constexpr int kLbGemmKChunk = 64;
+
 // window statistics: one block per 32 segments, warp 0 runs the running sums
 // and warps 1-3 derive mean and sigma
 constexpr int kMvmeanThreads = 128;
@@ -99,6 +131,18 @@ template <int METRIC, bool GW>
 __global__ void k_dp(Geom g, DpJob job);
 // the DP kernel for a metric, with its band in shared memory or in job.gwork
 const void* dp_kernel(int metric, bool gw);
+// wide-band DP: one warp per candidate, one anti-diagonal per step, the band
+// in registers (K chunks of 64 band offsets per warp, 2w+1 <= 64 K)
+template <int METRIC, int K>
+__global__ void k_dpw(Geom g, DpJob job);
+constexpr int kDpwThreads = 128;
+constexpr int kDpwMaxChunks = 8;  // w <= 255
+// the wavefront kernel for (metric, w), or null when the band is too wide
+const void* dpw_kernel(int metric, int w);
+// shared memory: the query plus, per warp, its candidate and the row-block
+// suffix sums of the abandon bound
+__host__ __device__ size_t dpw_warp_doubles(int m);
+size_t dpw_smem_bytes(int m, int warps);
 __global__ void k_lb_filter(Geom g, const double* __restrict__ z, const double* __restrict__ SIG,
                             const double* __restrict__ cutoff, int metric, long long* out,
                             unsigned long long* n_out, long long cap);

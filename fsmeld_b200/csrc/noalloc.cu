@@ -12,16 +12,22 @@
 // loads the library holds until the process exits.
 //
 // Limits: at most FSMELD_NOALLOC_MAX_WINDOWS windows (n - m + 1) and
-// m <= FSMELD_NOALLOC_MAX_M per call; the DP band must fit shared memory.
+// m <= FSMELD_NOALLOC_MAX_M per call; the DP band and candidate ring of the
+// lane-per-candidate DP must fit shared memory with the same 4 KB margin the
+// allocating path keeps, which on a 227 KB opt-in device means w <= 94.
 // Larger requests are rejected with FSMELD_E_ARG and a message.
 //
 // Set-up: the first call on a device looks up the array's device address with
 // cudaGetSymbolAddress while that device is current (a host-side reference to
-// the array is only a stand-in, not a device address).  Make that first call
-// before any stream capture.  Every call shares the one array and leaves its
-// contents behind; each call clears what must start at zero.  Calls whose
-// work overlaps on the GPU (different streams, or different host threads on
-// one device) race on the array: serialise them.
+// the array is only a stand-in, not a device address) and keeps it for the
+// life of the process, so the entry point must not be used on a device after
+// cudaDeviceReset in the same process.  Make that first call before any stream
+// capture.  The call is synchronous (it reads the match count back and waits
+// for its stream), so it must never be made while its stream is capturing.
+// The caller's current device is restored on return.  Every call shares the
+// one array and leaves its contents behind; each call clears what must start
+// at zero.  Calls whose work overlaps on the GPU (different streams, or
+// different host threads on one device) race on the array: serialise them.
 #include <algorithm>
 #include <cmath>
 #include <mutex>
@@ -110,10 +116,9 @@ __global__ void __launch_bounds__(1024) k_noalloc_compact(const double* __restri
 
 using namespace fsm;
 
-extern "C" int fsmeld_exact_noalloc(int device, const double* device_target, int64_t n, const double* host_query,
-                                    int m, int metric, int w, double arg, double cutoff, int64_t* device_out_idx,
-                                    double* device_out_dist, int64_t capacity, int64_t* host_out_count,
-                                    void* stream) {
+static int exact_noalloc(int device, const double* device_target, int64_t n, const double* host_query, int m,
+                         int metric, int w, double arg, double cutoff, int64_t* device_out_idx,
+                         double* device_out_dist, int64_t capacity, int64_t* host_out_count, void* stream) {
     if (!device_target || !host_query || !device_out_idx || !device_out_dist || !host_out_count || capacity < 0)
         return fail(FSMELD_E_ARG, "fsmeld_exact_noalloc: null pointer or negative capacity");
     if (device < 0 || device >= 256) return fail(FSMELD_E_ARG, "fsmeld_exact_noalloc: bad device index");
@@ -182,7 +187,7 @@ extern "C" int fsmeld_exact_noalloc(int device, const double* device_target, int
     int dev_optin = 0;
     if ((e = cudaDeviceGetAttribute(&dev_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device)) != cudaSuccess)
         return cuda_fail(e, "cudaDeviceGetAttribute", __FILE__, __LINE__);
-    if (smem > (size_t)dev_optin)
+    if (smem > (size_t)dev_optin - 4096)
         return fail(FSMELD_E_ARG, "fsmeld_exact_noalloc: band 2w+1 too wide for shared memory on this path");
     int sms = 0;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
@@ -230,4 +235,17 @@ extern "C" int fsmeld_exact_noalloc(int device, const double* device_target, int
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize", __FILE__, __LINE__);
     *host_out_count = (int64_t)total;
     return FSMELD_OK;
+}
+
+extern "C" int fsmeld_exact_noalloc(int device, const double* device_target, int64_t n, const double* host_query,
+                                    int m, int metric, int w, double arg, double cutoff, int64_t* device_out_idx,
+                                    double* device_out_dist, int64_t capacity, int64_t* host_out_count,
+                                    void* stream) {
+    int prev = -1;
+    const cudaError_t e = cudaGetDevice(&prev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice", __FILE__, __LINE__);
+    const int r = exact_noalloc(device, device_target, n, host_query, m, metric, w, arg, cutoff, device_out_idx,
+                                device_out_dist, capacity, host_out_count, stream);
+    if (prev != device) cudaSetDevice(prev);
+    return r;
 }

@@ -43,6 +43,13 @@ int device_index() {
     return d ? std::atoi(d) : 0;
 }
 
+// FSMELD_NORMALIZATION=raw selects the raw mode (fsmeld_set_normalization);
+// the reference's command line always runs z-score (src/main.cpp:89)
+bool raw_mode() {
+    const char* v = std::getenv("FSMELD_NORMALIZATION");
+    return v != nullptr && std::string(v) == "raw";
+}
+
 bool quiet_matches() {  // src/fsmeld.cpp:998-1001
     const char* v = std::getenv("FSMELD_QUIET_MATCHES");
     return v != nullptr && std::string(v) != "0" && std::string(v) != "false";
@@ -106,7 +113,7 @@ void emit_csv(const Row& r) {  // src/search_result.cpp:39-101
         "invalid_candidates,pruned_candidates,pruning_rate,survivors,matches,"
         "lbip_time,lbip_pruning_rate,timestamp";
     const double rate = r.valid == 0 ? 0.0 : (double)r.pruned / (double)r.valid;
-    std::string row = csv_escape(r.dataset) + ",zscore," + csv_escape(r.metric) + "," +
+    std::string row = csv_escape(r.dataset) + (raw_mode() ? ",raw," : ",zscore,") + csv_escape(r.metric) + "," +
                       std::to_string(r.m) + "," + std::to_string(r.w) + "," + g17(r.xi) + "," +
                       csv_escape(r.method) + "," + g17(r.lb_time) + "," + g17(r.total_time) + "," +
                       std::to_string(r.valid) + "," + std::to_string(r.invalid) + "," +
@@ -146,6 +153,19 @@ int setup(const char* tp, const char* qp, int m, Setup* s) {
         return r;
     }
     s->n = fsmeld_target_length(s->ctx);
+    if (raw_mode()) fsmeld_set_normalization(s->ctx, FSMELD_NORM_RAW);
+    // FSMELD_TUNE_TABLE: a tuning table file (fsmeld_set_tuning) for the kernel choices
+    if (const char* tp_env = std::getenv("FSMELD_TUNE_TABLE")) {
+        if (FILE* tf = fopen(tp_env, "r")) {
+            std::string text;
+            char buf[4096];
+            size_t got;
+            while ((got = fread(buf, 1, sizeof(buf), tf)) > 0) text.append(buf, got);
+            fclose(tf);
+            if (fsmeld_set_tuning(s->ctx, text.c_str()))
+                fprintf(stderr, "[Warning] %s\n", fsmeld_last_error(s->ctx));
+        }
+    }
     if (!read_query(qp, m, &s->q)) {
         fprintf(stderr, "Error: Query must begin with m finite numeric values.\n");
         return FSMELD_E_ARG;

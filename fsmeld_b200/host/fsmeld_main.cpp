@@ -3,6 +3,7 @@
 // error messages ("Error: ..." on stderr, exit status 1) and dispatch; the
 // work is done by the C ABI (include/fsmeld_cuda.h).
 #include <cmath>
+#include <cstdlib>
 #include <filesystem>
 #include <fstream>
 #include <iostream>
@@ -85,7 +86,12 @@ int main(int argc, char** argv) {
         }
         const double mean = sum / m;
         const double sigma = std::sqrt(squares / m - mean * mean);
-        if (!std::isfinite(sigma) || sigma <= 1e-12)
+        // FSMELD_NORMALIZATION=raw (no counterpart in the reference's command
+        // line, which always sets z-score, src/main.cpp:89): raw values, so a
+        // flat query is allowed
+        const char* norm = std::getenv("FSMELD_NORMALIZATION");
+        const bool raw = norm && std::string(norm) == "raw";
+        if (!raw && (!std::isfinite(sigma) || sigma <= 1e-12))
             throw std::invalid_argument(
                 "Query cannot be z-normalized: non-finite or near-zero standard deviation.");
         long long begin = -1, end = -1;

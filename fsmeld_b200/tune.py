@@ -1,0 +1,151 @@
+"""Measure the automatic kernel choices on the GPU and write the tuning table.
+
+Two choices depend on the shape and are settled by measurement:
+
+* the exact DP kernel (`dp` rules): the lane-per-candidate DP (band and
+  candidate ring per lane in shared memory) or the anti-diagonal wavefront
+  (one warp per candidate, band in registers), per metric, macro-segment
+  length m_k and radius w.  Timed as the exact scan (every window through the
+  DP, early abandon at the query's rank-20 distance) on a seeded random walk.
+* the LB_IP form of batched searches (`lb` rules): per-query thresholds and
+  FP64 FFTs, or one tensor-core product for the group, per metric, m_k and
+  group size.  Timed as one batched `search` of the group at each query's
+  rank-10 distance.
+
+Shapes where the lane DP's band does not fit shared memory need no
+measurement (the wavefront is the only shared-memory form there).  The table
+(fsmeld_b200/tune_table.txt) is loaded by api.Engine into every context.
+
+    python -m fsmeld_b200.tune [--quick] [--out PATH]
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import time
+
+import numpy as np
+
+from fsmeld_b200 import api
+from fsmeld_b200.synth import query_from, random_walk
+
+METRIC_ARGS = {"dtw": 0.0, "erp": 0.0, "edr": 0.25, "lcss": 0.25, "msm": 0.5}
+DP_SHAPES = {64: (2, 3, 6, 13, 31), 128: (3, 6, 13, 26, 51), 256: (6, 13, 26, 51, 94),
+             512: (13, 26, 51, 94), 1024: (26, 51, 94), 2048: (51, 94)}
+LB_SHAPES = {128: (2, 8, 32), 256: (2, 8, 32), 512: (2, 8, 32)}
+
+
+def macro_length(m):
+    mk = 1
+    while mk < 8 * m:
+        mk *= 2
+    return mk
+
+
+def lane_fits(w, smem_optin=232448):
+    ring = 1
+    while ring < 2 * w + 2:
+        ring *= 2
+    return 2 * 8 * 32 * (2 * w + 2 + ring) <= smem_optin - 4096
+
+
+def timed(eng, fn, reps=2):
+    fn()  # warm-up (workspace)
+    best = float("inf")
+    for _ in range(reps):
+        fn()
+        best = min(best, eng.last_call_ms)
+    return best
+
+
+def tune_dp(metrics, shapes, log):
+    rules = []
+    for m, ws in shapes.items():
+        n = (1 << 17) if m <= 256 else (1 << 16)
+        t = random_walk(n, 9000 + m)
+        q, _ = query_from(t, m, np.random.default_rng(9001 + m))
+        for metric in metrics:
+            arg = METRIC_ARGS[metric]
+            for w in ws:
+                if w >= m or not lane_fits(w):
+                    continue
+                times = {}
+                for form in ("lane", "wave"):
+                    table = f"dp {metric} {macro_length(m)} 1000 {form}\n"
+                    with api.Engine(t, tuning=table) as e:
+                        _, d, _ = e.cutoff(q, m, 20, metric, w, arg)
+                        cut = float(d[-1])
+                        times[form] = timed(e, lambda: e.exact(q, m, cut, metric, w, arg))
+                choice = min(times, key=times.get)
+                log(f"dp {metric} m={m} w={w}: lane {times['lane']:.2f} ms, wave {times['wave']:.2f} ms -> {choice}")
+                rules.append((metric, macro_length(m), w, choice, times))
+    return rules
+
+
+def tune_lb(metrics, shapes, log):
+    rules = []
+    t = random_walk(1 << 20, 9100)
+    for m, qcounts in shapes.items():
+        rng = np.random.default_rng(9101 + m)
+        w = max(1, m // 20)
+        for metric in metrics:
+            arg = METRIC_ARGS[metric]
+            with api.Engine(t, tuning="") as e:
+                qs = []
+                for _ in range(max(qcounts)):
+                    q, _ = query_from(t, m, rng)
+                    _, d, _ = e.cutoff(q, m, 10, metric, w, arg)
+                    qs.append(dict(query=q, m=m, metric=metric, w=w, arg=arg, cutoff=float(d[-1])))
+                for nq in qcounts:
+                    times = {}
+                    for form in ("fft", "gemm"):
+                        e.set_lb_form(form)
+                        times[form] = timed(e, lambda: e.batch("search", qs[:nq]))
+                    choice = min(times, key=times.get)
+                    log(f"lb {metric} m={m} q={nq}: fft {times['fft']:.2f} ms, gemm {times['gemm']:.2f} ms "
+                        f"-> {choice}")
+                    rules.append((metric, macro_length(m), nq, choice, times))
+    return rules
+
+
+def write_table(path, dp_rules, lb_rules):
+    lines = ["# Tuning table: measured by `python -m fsmeld_b200.tune` on one B200.",
+             "# kind metric m_k limit choice  (dp: w <= limit; lb: group size >= limit); first match wins"]
+    for metric, mk, w, choice, times in dp_rules:
+        lines.append(f"dp {metric} {mk} {w} {choice}   # lane {times['lane']:.2f} ms, wave {times['wave']:.2f} ms")
+    # lb: for each (metric, m_k) the smallest group size from which the product wins at every measured size
+    by_shape = {}
+    for metric, mk, nq, choice, times in lb_rules:
+        by_shape.setdefault((metric, mk), []).append((nq, choice, times))
+    for (metric, mk), rows in by_shape.items():
+        rows.sort()
+        qmin = None
+        for i, (nq, _, _) in enumerate(rows):
+            if all(ch == "gemm" for _, ch, _ in rows[i:]):
+                qmin = nq
+                break
+        detail = ", ".join(f"q={nq}: fft {tm['fft']:.1f} / gemm {tm['gemm']:.1f} ms" for nq, _, tm in rows)
+        if qmin is not None:
+            lines.append(f"lb {metric} {mk} {qmin} gemm   # {detail}")
+        else:
+            lines.append(f"# lb {metric} {mk}: fft at every measured size ({detail})")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=api.TUNE_TABLE)
+    ap.add_argument("--quick", action="store_true", help="DTW and MSM only")
+    args = ap.parse_args()
+    metrics = ["dtw", "msm"] if args.quick else list(METRIC_ARGS)
+    t0 = time.time()
+    log = lambda s: print(s, flush=True)  # noqa: E731
+    dp = tune_dp(metrics, DP_SHAPES, log)
+    lb = tune_lb(metrics, LB_SHAPES, log)
+    write_table(args.out, dp, lb)
+    log(f"wrote {args.out} in {time.time() - t0:.0f} s")
+
+
+if __name__ == "__main__":
+    main()

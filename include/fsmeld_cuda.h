@@ -116,6 +116,44 @@ const char* fsmeld_strerror(int status);
  * counterpart (the reference runs one query per process). */
 int fsmeld_set_concurrency(fsmeld_ctx* ctx, int queries);
 
+/* Normalisation mode of the context's queries (include/funcs.h:20-28,
+ * src/normalization_mode.cpp:7-21: set_normalization_mode /
+ * normalization_mode).  FSMELD_NORM_ZSCORE (default; the only mode the
+ * reference's command line sets, src/main.cpp:89) z-normalises the query and
+ * every candidate window.  FSMELD_NORM_RAW compares raw values: the query is
+ * used as given (a flat query is allowed) and every window whose points are
+ * all finite is a candidate, flat windows included.  The reference declares
+ * the raw mode but never consults it; here it runs the same cascade on raw
+ * values (window mean 0, sigma 1). */
+#define FSMELD_NORM_ZSCORE 0
+#define FSMELD_NORM_RAW 1
+int fsmeld_set_normalization(fsmeld_ctx* ctx, int mode);
+int fsmeld_normalization(const fsmeld_ctx* ctx);
+
+/* LB_IP form of batched searches (fsmeld_batch, mode 0) whose queries share
+ * (m, w) and metric (no reference counterpart; the reference computes LB_IP
+ * per query with FFTs, src/sip.cpp:16-52).  FSMELD_LB_FFT: per query and
+ * segment, the reference's threshold selection and an FP64 FFT.
+ * FSMELD_LB_GEMM: one threshold pair for the group and the sliding inner
+ * products of all its queries as one tensor-core product (BF16x3 split, FP32
+ * accumulation, each bound lowered by its rounding-error margin).  Match
+ * sets are the same either way; the LB_IP survivor counters differ.
+ * FSMELD_LB_AUTO (default): the tuner's choice for the group's shape. */
+#define FSMELD_LB_AUTO 0
+#define FSMELD_LB_FFT 1
+#define FSMELD_LB_GEMM 2
+int fsmeld_set_lb_form(fsmeld_ctx* ctx, int form);
+
+/* Tuning table for the automatic choices (no reference counterpart): one rule
+ * per line, "kind metric m_k limit choice", first match wins, '#' comments.
+ *   dp <metric> <m_k> <w_max>  lane|wave   exact DP kernel for w <= w_max
+ *   lb <metric> <m_k> <q_min>  fft|gemm    LB_IP form for groups of >= q_min
+ * Shapes no rule covers keep the built-in choice (the lane DP while its band
+ * fits shared memory; the FFT LB_IP).  fsmeld_b200/tune.py measures the
+ * rules on the GPU and writes fsmeld_b200/tune_table.txt, which the Python
+ * binding loads into every context. */
+int fsmeld_set_tuning(fsmeld_ctx* ctx, const char* table);
+
 /* Cap on device workspace bytes (0 = no cap); exceeding it -> FSMELD_E_NOMEM. */
 int fsmeld_set_workspace_limit(fsmeld_ctx* ctx, int64_t bytes);
 /* Number of CUDA kernel launches issued by this context so far. */
@@ -154,7 +192,9 @@ int fsmeld_batch(fsmeld_ctx* ctx, int mode, const fsmeld_query* queries, int nq,
  * arrays of one query, for stage-by-stage comparison with a CPU model.
  * what: 0 window means [S*kml], 1 window sigmas [S*kml], 2 U_normal
  * [S*m_k], 3 L_normal [S*m_k], 4 thresholds (t_l, t_u) [2*S], 5 LB_IP per
- * window [S*kml] (NaN for invalid windows); S counts the tail segment.
+ * window [S*kml] (NaN for invalid windows), 6 LB_IP per window through the
+ * tensor-core form (fsmeld_set_lb_form) with this query as the group, 7 the
+ * (t_l, t_u, margin_l, margin_u) that form used; S counts the tail segment.
  * Returns the number of doubles available (copies at most cap). ---- */
 int64_t fsmeld_inspect(fsmeld_ctx* ctx, const double* query, int m, int metric, int w, double arg,
                        int what, double* out, int64_t cap);
@@ -171,10 +211,14 @@ int64_t fsmeld_inspect(fsmeld_ctx* ctx, const double* query, int m, int metric, 
  * cudaStream_t, NULL for the default stream) and returns after it finishes.
  * Scratch is one static device array of 12 MiB per GPU, held until exit.
  * Limits: n - m + 1 <= FSMELD_NOALLOC_MAX_WINDOWS, m <= FSMELD_NOALLOC_MAX_M,
- * and the DP band (2w+1) must fit shared memory; larger requests return
- * FSMELD_E_ARG with a message.  The first call on a device looks up the
- * scratch array's device address: make it before any stream capture.  Calls
- * share the array: calls that overlap on the GPU race, so serialise them. */
+ * and the DP band (2w+1) must fit shared memory (w <= 94 on a 227 KB opt-in
+ * device); larger requests return FSMELD_E_ARG with a message.  The first
+ * call on a device looks up the scratch array's device address and keeps it
+ * for the process: make it before any stream capture, and do not use the
+ * entry point on a device after cudaDeviceReset.  The call is synchronous and
+ * must never be made while its stream is capturing.  It restores the caller's
+ * current device.  Calls share the array: calls that overlap on the GPU race,
+ * so serialise them. */
 #define FSMELD_NOALLOC_MAX_WINDOWS 262144
 #define FSMELD_NOALLOC_MAX_M 2048
 int fsmeld_exact_noalloc(int device, const double* device_target, int64_t n, const double* host_query, int m,

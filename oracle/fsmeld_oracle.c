@@ -865,8 +865,22 @@ double orc_distance(int metric, const double* q, const double* t, int m, int w, 
 
 /* --------------------------------------------------------------- drivers */
 
+/* Normalisation mode (include/funcs.h:20-28, src/normalization_mode.cpp):
+ * 0 z-score, the reference command line's only mode; 1 raw.  The reference
+ * declares the raw mode but never consults it, so its raw behaviour is this
+ * restatement's own definition (parity unpinned): the query is used as
+ * given, a window is valid iff its points are all finite, and its
+ * statistics are mean 0 and sigma 1, so (t - 0) / 1 leaves candidates and
+ * envelopes as they are and the cascade runs unchanged on raw values. */
+static int g_orc_raw = 0;
+void orc_set_normalization(int raw) { g_orc_raw = raw != 0; }
+
 /* src/fsmeld.cpp:622-639 */
 void orc_normalize_query(const double* q, int m, double* qn) {
+    if (g_orc_raw) {
+        memcpy(qn, q, sizeof(double) * (size_t)m);
+        return;
+    }
     double ex = 0, ex2 = 0;
     for (int i = 0; i < m; i++) { ex += q[i]; ex2 += q[i] * q[i]; }
     const double mean = ex / m;
@@ -926,6 +940,15 @@ static void seg_free(orc_seg* s) {
  * src/fsmeld.cpp:753-755 / 861-864 and the exclusion at 131-152. */
 static void seg_stats(orc_seg* s, const double* t, int first, int count, long long gstart) {
     orc_mvmean(t, s->m_k, s->m, s->miu, s->si);
+    if (g_orc_raw) {  /* raw mode: (0, 1) for windows of finite points, NaN otherwise */
+        int bad = 0;
+        for (int k = 0; k < s->m; k++) bad += !isfinite(t[k]);
+        for (int j = 0; j + s->m <= s->m_k; j++) {
+            if (j > 0) bad += !isfinite(t[j + s->m - 1]) - !isfinite(t[j - 1]);
+            s->miu[j] = bad ? NAN : 0.0;
+            s->si[j] = bad ? NAN : 1.0;
+        }
+    }
     memset(s->invalid, 0, s->m_k);
     orc_invalid_mask(t, s->si, s->m_k, s->m, s->invalid);
     if (s->excl_b >= 0 && s->excl_e > s->excl_b) {

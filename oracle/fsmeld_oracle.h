@@ -45,7 +45,11 @@ double orc_glb(int metric, const double* Q, const double* T, int m, double arg,
                const double* LQ, const double* UQ, int w, double bsf);
 double orc_distance(int metric, const double* q, const double* t, int m, int w, double arg);
 
-/* query z-normalisation as src/fsmeld.cpp:622-639 (sum, sum of squares) */
+/* normalisation mode: 0 z-score (default), 1 raw (see fsmeld_oracle.c) */
+void orc_set_normalization(int raw);
+
+/* query z-normalisation as src/fsmeld.cpp:622-639 (sum, sum of squares);
+ * a copy in raw mode */
 void orc_normalize_query(const double* q, int m, double* q_normal);
 
 typedef struct {

@@ -17,7 +17,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_ORACLE = os.path.join(HERE, "liboracle.so")
 LIB_REF = os.path.join(HERE, "_ref", "libfsmeld_ref.so")
 BIN_REF = os.path.join(HERE, "_ref", "fsmeld_ref")
-REFERENCE_TREE = os.environ.get("FSMELD_REFERENCE_TREE", "/root/reference")
+# The reference source tree: $FSMELD_REFERENCE_TREE, else the folder
+# `reference` beside the repository.  Only build() reads it.
+REFERENCE_TREE = os.environ.get("FSMELD_REFERENCE_TREE") or os.path.normpath(
+    os.path.join(HERE, "..", "..", "reference"))
 
 METRICS = {"dtw": 1, "edr": 2, "erp": 3, "lcss": 4, "msm": 5}
 
@@ -109,6 +112,7 @@ class Oracle:
                                 C.POINTER(Counters))
             self._macro = L.fn("macro_length", C.c_int, C.c_int, C.c_longlong)
             self._normq = L.fn("normalize_query", None, _dp, C.c_int, _dp)
+            self._setnorm = L.fn("set_normalization", None, C.c_int)
         else:
             self._findt = L.fn("find_t", C.c_double, C.c_int, C.c_int, _dp, C.c_int, _dp, C.c_int,
                                C.c_double)
@@ -195,6 +199,12 @@ class Oracle:
         out = np.empty(len(q))
         self._normq(_ptr(q), len(q), _ptr(out))
         return out
+
+    def set_normalization(self, mode: str) -> None:
+        """'zscore' (default) or 'raw' for the restatement's drivers."""
+        if mode not in ("zscore", "raw"):
+            raise ValueError(mode)
+        self._setnorm(1 if mode == "raw" else 0)
 
     def search(self, target, query, m, cutoff, metric, w, arg, excl=(-1, -1), seg_counts=False):
         target, query = _d(target), _d(query)

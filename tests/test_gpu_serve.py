@@ -1,7 +1,8 @@
 """The serving loop on the CUDA path: a mix of search, cutoff and exact
 requests of several lengths, metrics and radii against two resident targets,
 submitted from three threads at once, must give exactly the answers of the
-same requests run alone (match lists and distances bit for bit, counters)."""
+same requests run alone on the GPU, and those of the oracle (match lists and
+distances bit for bit, counters)."""
 import threading
 
 import numpy as np
@@ -16,7 +17,7 @@ def _bits(a):
     return np.asarray(a, dtype=np.float64).view(np.int64)
 
 
-def test_mix_equals_alone():
+def test_mix_equals_alone(oracle):
     from fsmeld_b200 import api
     from fsmeld_b200.serve import Server
 
@@ -33,20 +34,24 @@ def test_mix_equals_alone():
         q, _ = query_from(targets[tname], m, rng)
         mode = ["search", "cutoff", "exact"][i % 3]
         reqs.append((tname, mode, q, m, metric, w, arg))
-    # cutoffs for search/exact: each query's k=8 distance, from a plain engine
-    alone = {}
+    # cutoffs for search/exact: each query's k=8 distance from the oracle;
+    # every request's answer from the oracle and from a plain engine alone
+    alone, want = {}, {}
     with api.Engine(targets["a"]) as ea, api.Engine(targets["b"]) as eb:
         eng = {"a": ea, "b": eb}
         for j, (tn, mode, q, m, metric, w, arg) in enumerate(reqs):
-            e = eng[tn]
-            _, d8, _ = e.cutoff(q, m, 8, metric, w, arg)
+            e, t = eng[tn], targets[tn]
+            _, d8, _ = oracle.cutoff(t, q, m, 8, metric, w, arg)
             cut = float(d8[-1])
             if mode == "search":
                 alone[j] = (cut, e.search(q, m, cut, metric, w, arg))
+                want[j] = oracle.search(t, q, m, cut, metric, w, arg)
             elif mode == "exact":
                 alone[j] = (cut, e.exact(q, m, cut, metric, w, arg))
+                want[j] = oracle.exact(t, q, m, cut, metric, w, arg)
             else:
                 alone[j] = (None, e.cutoff(q, m, 5, metric, w, arg))
+                want[j] = oracle.cutoff(t, q, m, 5, metric, w, arg)
     with Server(device=0) as srv:
         for name, t in targets.items():
             srv.add_target(name, t)
@@ -69,9 +74,13 @@ def test_mix_equals_alone():
             x.join()
         for j, f in sorted(futs.items()):
             got = f.result(timeout=120)
-            ref = alone[j][1]
-            assert list(got[0]) == list(ref[0]), j
+            ref, orc = alone[j][1], want[j]
+            assert list(got[0]) == list(ref[0]) == list(orc[0]), j
             if len(ref) == 3:
                 assert np.array_equal(_bits(got[1]), _bits(ref[1])), j
+                assert np.array_equal(_bits(got[1]), _bits(orc[1])), j
             for key in ("valid", "invalid", "after_lb", "after_glb", "matches"):
                 assert got[-1][key] == ref[-1][key], (j, key)
+            keys = ("valid", "invalid", "after_lb", "after_glb", "matches") if reqs[j][1] == "search" else ("valid",)
+            for key in keys:
+                assert got[-1][key] == orc[-1][key], (j, key)

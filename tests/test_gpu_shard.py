@@ -2,8 +2,8 @@
 
 Every rank's slice is searched by an `api.Engine` that borrows the device
 memory of one resident copy of the target (slice starts are 8-byte aligned
-only); the merged results must equal one search over the whole target, bit
-for bit, with summed counters.  The ranks run one after another in this
+only); the merged results must equal the oracle over the whole target and
+one engine over the whole target, bit for bit, with summed counters.  The ranks run one after another in this
 process (the merge is the same host code the collective calls use)."""
 import numpy as np
 import pytest
@@ -21,7 +21,7 @@ def _bits(a):
 
 
 @pytest.mark.parametrize("world", [2, 3])
-def test_sharded_engine_equals_whole_target(world):
+def test_sharded_engine_equals_whole_target(oracle, world):
     import torch
 
     from fsmeld_b200 import api
@@ -48,6 +48,8 @@ def test_sharded_engine_equals_whole_target(world):
                     [r.local_cutoff(q, m, 20, metric, w, arg) for r in ranks], m, n, 20)
                 assert list(sidx) == list(fidx) and np.array_equal(_bits(sdist), _bits(fdist)), metric
                 assert sc["valid"] == fc["valid"]
+                kidx, kdist, _ = oracle.cutoff(t, q, m, 20, metric, w, arg)
+                assert list(sidx) == list(kidx) and np.array_equal(_bits(sdist), _bits(kdist)), metric
                 cut = float(fdist[-1])
                 oidx, oc = full.search(q, m, cut, metric, w, arg)
                 gidx, gc = ShardedSearch.merge_search([r.local_search(q, m, cut, metric, w, arg) for r in ranks],
@@ -55,10 +57,16 @@ def test_sharded_engine_equals_whole_target(world):
                 assert list(gidx) == list(oidx), metric
                 for key in ("valid", "invalid", "after_lb", "after_glb", "matches", "segments", "tail", "m_k"):
                     assert gc[key] == oc[key], (metric, key)
+                yidx, yc = oracle.search(t, q, m, cut, metric, w, arg)
+                assert list(gidx) == list(yidx), metric
+                for key in ("valid", "invalid", "after_lb", "after_glb", "matches"):
+                    assert gc[key] == yc[key], (metric, key)
                 eidx, edist, _ = full.exact(q, m, cut, metric, w, arg)
                 xidx, xdist, _ = ShardedSearch.merge_exact([r.local_exact(q, m, cut, metric, w, arg) for r in ranks],
                                                            m, n, cut)
                 assert list(xidx) == list(eidx) and np.array_equal(_bits(xdist), _bits(edist)), metric
+                zidx, zdist, _ = oracle.exact(t, q, m, cut, metric, w, arg)
+                assert list(xidx) == list(zidx) and np.array_equal(_bits(xdist), _bits(zdist)), metric
                 pidx, pc = full.search(q, m, cut, metric, w, arg, exclude=excl)
                 hidx, hc = ShardedSearch.merge_search(
                     [r.local_search(q, m, cut, metric, w, arg, exclude=excl) for r in ranks], m, n, cut)

@@ -1,7 +1,7 @@
 """A target file streamed through the GPU in segment-aligned chunks (two
-engines alternating, uploads from pinned memory) gives the results of one
-engine over the whole target, bit for bit, for a batch of queries of two
-lengths."""
+engines alternating, uploads from pinned memory) gives the results of the
+oracle over the whole target and of one resident engine, bit for bit, for a
+batch of queries of two lengths."""
 import os
 import tempfile
 
@@ -17,7 +17,7 @@ def _bits(a):
     return np.asarray(a, dtype=np.float64).view(np.int64)
 
 
-def test_streamed_equals_resident():
+def test_streamed_equals_resident(oracle):
     from fsmeld_b200 import api
     from fsmeld_b200.stream import StreamingTarget, chunk_plan
 
@@ -30,18 +30,26 @@ def test_streamed_equals_resident():
         m = 64 if i % 2 else 96
         q, _ = query_from(t, m, rng)
         qs.append(dict(query=q, m=m, metric=metric, w=5, arg=arg))
+    for d in qs:
+        _, dk, _ = oracle.cutoff(t, d["query"], d["m"], 12, d["metric"], d["w"], d["arg"])
+        d["cutoff"] = float(dk[-1])
+    orc = {"search": [oracle.search(t, d["query"], d["m"], d["cutoff"], d["metric"], d["w"], d["arg"]) for d in qs],
+           "exact": [oracle.exact(t, d["query"], d["m"], d["cutoff"], d["metric"], d["w"], d["arg"]) for d in qs],
+           "cutoff": [oracle.cutoff(t, d["query"], d["m"], 12, d["metric"], d["w"], d["arg"]) for d in qs]}
     with api.Engine(t) as full:
-        for d in qs:
-            _, dk, _ = full.cutoff(d["query"], d["m"], 12, d["metric"], d["w"], d["arg"])
-            d["cutoff"] = float(dk[-1])
         want = {mode: full.batch(mode, [dict(d, k=12) if mode == "cutoff" else d for d in qs])
                 for mode in ("search", "exact", "cutoff")}
     with StreamingTarget(path, max_points=40_000) as st:
         assert len(chunk_plan(len(t), 96, 40_000)) >= 6
         for mode in ("search", "exact", "cutoff"):
             got = st.batch(mode, [dict(d, k=12) if mode == "cutoff" else d for d in qs])
-            for g, w_ in zip(got, want[mode]):
-                assert list(g["idx"]) == list(w_["idx"]), mode
+            for g, w_, o in zip(got, want[mode], orc[mode]):
+                assert list(g["idx"]) == list(w_["idx"]) == list(o[0]), mode
+                if mode != "search":
+                    assert np.array_equal(_bits(g["dist"]), _bits(o[1])), mode
+                else:
+                    for key in ("valid", "invalid", "after_lb", "after_glb", "matches"):
+                        assert g["counters"][key] == o[1][key], (mode, key)
                 if mode != "search":
                     assert np.array_equal(_bits(g["dist"]), _bits(w_["dist"])), mode
                 if mode == "search":
