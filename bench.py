@@ -488,10 +488,13 @@ C4_M, C4_W, C4_KS = 512, 26, (10, 100)
 
 def workload_c4(args):
     """Many DTW top-k queries (m=512, w=26, k=10 and 100) over one 2^27-point
-    walk with bursts: queries/s of the batched device-resident `cutoff`.  Each
-    measured ranking is checked against an independent path on a 2^22-point
-    prefix: the exact scan (every window through the DP) at the returned
-    threshold must give the same k smallest (distance, index) pairs."""
+    walk with bursts: queries/s of the batched device-resident `cutoff`, with
+    LB_IP per query by FFT and for the whole group as one tensor-core product
+    (the rankings of the two must be identical).  A consistency check on a
+    2^22-point prefix: the exact scan (every window through the DP) at the
+    returned threshold must give the same k smallest (distance, index) pairs
+    (the rankings against the oracle, ties included, are checked by the GPU
+    tests)."""
     import torch
 
     from fsmeld_b200 import api
@@ -503,20 +506,33 @@ def workload_c4(args):
     qs = [query_from(t, C4_M, rng)[0] for _ in range(args.queries)]
     eng = api.Engine(t)
     out = {}
+    forms = {}
     for k in C4_KS:
         batch = [dict(query=q, m=C4_M, metric="dtw", w=C4_W, arg=0.0, k=k) for q in qs]
-        eng.batch("cutoff", batch[:2])  # warm-up (workspace, statistics)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        res = eng.batch("cutoff", batch)
-        wall = time.perf_counter() - t0
-        dev_ms = eng.last_call_ms
-        bad = [r["status"] for r in res if r["status"] != 0]
-        if bad:
-            raise RuntimeError(f"cutoff failed: {bad}")
-        out[k] = {"queries": len(qs), "device_ms": round(dev_ms, 2), "queries_per_s": len(qs) / (dev_ms / 1e3),
-                  "wall_queries_per_s": len(qs) / wall,
-                  "mean_threshold": float(np.mean([r["counters"]["threshold"] for r in res]))}
+        per_form = {}
+        ranks = {}
+        for form in ("fft", "gemm"):
+            eng.set_lb_form(form)
+            eng.batch("cutoff", batch[:2])  # warm-up (workspace, statistics)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = eng.batch("cutoff", batch)
+            wall = time.perf_counter() - t0
+            dev_ms = eng.last_call_ms
+            bad = [r["status"] for r in res if r["status"] != 0]
+            if bad:
+                raise RuntimeError(f"cutoff failed ({form}): {bad}")
+            ranks[form] = [(list(r["idx"]), np.asarray(r["dist"]).view(np.int64).tolist()) for r in res]
+            per_form[form] = {"device_ms": round(dev_ms, 2), "queries_per_s": len(qs) / (dev_ms / 1e3),
+                              "wall_queries_per_s": len(qs) / wall,
+                              "lb_survivors_mean": float(np.mean([r["counters"]["after_lb"] for r in res]))}
+        if ranks["fft"] != ranks["gemm"]:
+            raise RuntimeError("c4: rankings of the two LB_IP forms differ")
+        best = max(per_form, key=lambda f: per_form[f]["queries_per_s"])
+        out[k] = dict(per_form[best], queries=len(qs), lb_form=best,
+                      mean_threshold=float(np.mean([r["counters"]["threshold"] for r in res])))
+        forms[k] = per_form
+    eng.set_lb_form("auto")
     # independent check on a prefix: cutoff ranking == k smallest of the exact scan at its threshold
     pre = t[:1 << 22]
     checked = 0
@@ -536,7 +552,8 @@ def workload_c4(args):
             "higher_is_better": True, "dtype": "f64", "data": "synthetic (seeded random walk with bursts)",
             "config": {"workload": f"c4: {len(qs)} DTW top-k queries, m={C4_M}, w={C4_W}, k=10 and k=100, "
                                    f"n={n} walk + bursts on 1% of points (N(0,5))", "n": n},
-            "per_k": out, "rankings_checked_against_exact_scan": checked,
+            "per_k": out, "lb_forms": forms, "rankings_identical_across_lb_forms": True,
+            "rankings_checked_against_exact_scan": checked,
             "hbm_peak_gbs": peaks["hbm_gbs"]}
     print(json.dumps(line))
     return 0
@@ -655,7 +672,8 @@ def workload_c5(args):
     from fsmeld_b200.serve import Server
     from fsmeld_b200.synth import query_from, random_walk
 
-    sizes = {"t24": 1 << 24, "t22": 1 << 22}  # 2^28 / 2^25 scaled down to bound the run
+    big, small = args.c5_log2
+    sizes = {f"t{big}": 1 << big, f"t{small}": 1 << small}  # the stated 2^28 and 2^25 by default
     targets = {name: random_walk(n, seed=50 + i) for i, (name, n) in enumerate(sizes.items())}
     rng = np.random.default_rng(505)
     metrics = [("dtw", 0.0), ("erp", 0.0), ("edr", 0.25), ("lcss", 0.25), ("msm", 0.5)]
@@ -729,10 +747,11 @@ def workload_c5(args):
     lat_ms = np.asarray([x for x in lat if x is not None]) * 1e3
     line = {"metric": "requests/s", "value": len(reqs) / span, "unit": "requests/s", "n_gpus": 1,
             "higher_is_better": True, "dtype": "f64", "data": "synthetic (seeded random walks)",
-            "config": {"workload": f"c5 serving: {len(reqs)} search requests, Poisson arrivals at "
-                                   f"{args.rate}/s, targets 2^24 and 2^22 points resident, m log-uniform "
-                                   "[64, 2048], metric uniform, w uniform [0, 0.1 m], cutoff = rank "
-                                   "ceil(1e-4 (n-m+1)) distance", "rate_per_s": args.rate},
+            "config": {"workload": f"c5 serving: {len(reqs)} search requests (a sample of the 20k-request "
+                                   f"stream), Poisson arrivals at {args.rate}/s, targets 2^{big} and 2^{small} "
+                                   "points resident, m log-uniform [64, 2048], metric uniform, w uniform "
+                                   "[0, 0.1 m], cutoff = rank ceil(1e-4 (n-m+1)) distance",
+                       "rate_per_s": args.rate, "requests": len(reqs)},
             "latency_ms": {"p50": round(float(np.percentile(lat_ms, 50)), 2),
                            "p99": round(float(np.percentile(lat_ms, 99)), 2),
                            "max": round(float(lat_ms.max()), 2)},
@@ -798,6 +817,8 @@ def main():
                          "c4: batched DTW top-k queries over a 2^27-point target (queries/s); "
                          "c5: serving loop with Poisson arrivals (latency)")
     ap.add_argument("--rate", type=float, default=50.0, help="c5: request arrivals per second")
+    ap.add_argument("--c5-log2", type=int, nargs=2, default=(28, 25),
+                    help="c5: log2 sizes of the two resident targets (stated: 28 25)")
     ap.add_argument("--queries", type=int, default=32, help="c4: number of queries (c3: 512 unless given)")
     ap.add_argument("--dropin-sample", type=int, default=8,
                     help="c3: queries timed through the plain drop-in command, one process each")

@@ -769,86 +769,18 @@ static int search_tail(fsmeld_ctx* c, const Geom& g, const QueryDev& qd, const S
     return FSMELD_OK;
 }
 
-static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& st, bool have_env) {
+// The top-k after LB_IP: per-segment seeds by bound z (NaN: invalid), the
+// k-th seed distance tau selected on the device, the LB filter, GLB and the
+// exact DP at tau, ordered (distance, index) results and counters.
+static int cutoff_tail(fsmeld_ctx* c, const Geom& g, const QueryDev& qd, const Stats& st, double* z,
+                       unsigned long long* cnt, const QueryRun& qr) {
     int r;
-    Geom g = g0;
-    g.excl_b = (qr.eb >= 0 && qr.ee > qr.eb) ? qr.eb : -1;
-    g.excl_e = (qr.eb >= 0 && qr.ee > qr.eb) ? qr.ee : -1;
-    const HostQuery& hq = *qr.hq;
-    QueryDev qd;
-    if ((r = upload_query(c, hq, "query", &qd))) return r;
-    unsigned long long* cnt;
-    if ((r = bufT(c, "counters", C_N, &cnt))) return r;
-    FSM_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, c->stream));
     const long long cap = g.tsn;
     unsigned long long h[C_N] = {0};
     fsmeld_counters out{};
     out.m_k = g.m_k;
     out.segments = g.forsize;
     out.tail = g.tsn % g.kml;
-
-    if (qr.mode == 2) {  // exact: every valid window through the DP
-        long long *oi;
-        double* od;
-        if ((r = bufT(c, "outi", (size_t)cap, &oi))) return r;
-        if ((r = bufT(c, "outd", (size_t)cap, &od))) return r;
-        qd.cutoff = qr.cutoff;
-        DpJob dj{};
-        dj.q = qd; dj.target = c->d_target; dj.MU = st.MU; dj.SIG = st.SIG;
-        dj.list = nullptr; dj.n_windows = g.tsn; dj.mode = 0; dj.cutoff = qr.cutoff;
-        dj.out_idx = oi; dj.out_dist = od; dj.n_out = cnt + C_OUT; dj.n_cells = cnt + C_CELLS; dj.out_cap = cap; dj.n_valid = cnt + C_VALID;
-        if ((r = run_dp(c, g, dj, g.tsn))) return r;
-        FSM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
-        FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
-        const long long nout = (long long)h[C_OUT];
-        if ((r = sort_pairs_i64(c, oi, od, nout))) return r;
-        const long long ncopy = std::min<long long>(nout, qr.cap);
-        if (ncopy > 0) {
-            FSM_CUDA_TRY(cudaMemcpyAsync(qr.out_idx, oi, sizeof(long long) * ncopy, cudaMemcpyDeviceToHost, c->stream));
-            if (qr.out_dist) FSM_CUDA_TRY(cudaMemcpyAsync(qr.out_dist, od, sizeof(double) * ncopy, cudaMemcpyDeviceToHost, c->stream));
-        }
-        FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
-        out.valid = (long long)h[C_VALID];
-        out.invalid = g.tsn - out.valid;
-        out.after_lb = out.after_glb = out.exact_evals = out.valid;
-        out.matches = nout;
-        out.dp_cells = (long long)h[C_CELLS];
-        out.threshold = qr.cutoff;
-        if (qr.out_count) *qr.out_count = nout;
-        if (qr.cnt) *qr.cnt = out;
-        return FSMELD_OK;
-    }
-
-    // thresholds
-    double* thr;
-    if ((r = bufT(c, "thr", (size_t)2 * g.S, &thr))) return r;
-    std::vector<ThrJob> jobs(1);
-    jobs[0].q = qd; jobs[0].Un = st.Un; jobs[0].Ln = st.Ln; jobs[0].thr = thr;
-    if ((r = run_thr(c, g, jobs))) return r;
-    (void)have_env;
-
-    long long* segc = nullptr;
-    if ((r = bufT(c, "segc", (size_t)3 * g.S, &segc))) return r;
-
-    if (qr.mode == 0) {  // search
-        long long* surv;
-        if ((r = bufT(c, "surv", (size_t)cap, &surv))) return r;
-        qd.cutoff = qr.cutoff;
-        LbJob lj{};
-        lj.q = qd; lj.Un = st.Un; lj.Ln = st.Ln; lj.thr = thr; lj.SIG = st.SIG;
-        lj.zout = nullptr; lj.surv = surv; lj.surv_cap = cap; lj.nsurv = cnt + C_SURV;
-        lj.nvalid = cnt + C_VALID; lj.segc = segc;
-        if ((r = run_lbip(c, g, lj))) return r;
-        return search_tail(c, g, qd, st, surv, cnt, cap, segc, qr);
-    }
-
-    // cutoff (top-k)
-    double* z;
-    if ((r = bufT(c, "zbuf", (size_t)g.S * g.kml, &z))) return r;
-    LbJob lj{};
-    lj.q = qd; lj.Un = st.Un; lj.Ln = st.Ln; lj.thr = thr; lj.SIG = st.SIG;
-    lj.zout = z; lj.surv = nullptr; lj.nsurv = cnt + C_SURV; lj.nvalid = cnt + C_VALID; lj.segc = nullptr;
-    if ((r = run_lbip(c, g, lj))) return r;
     // seeds
     // seeds per segment: enough for k of them (2k over all segments), at most 32
     const int per_seg = (int)std::min<long long>(32, std::max<long long>(1, (2 * qr.k + g.S - 1) / g.S));
@@ -936,6 +868,89 @@ static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& s
     return FSMELD_OK;
 }
 
+static int run_query(fsmeld_ctx* c, const QueryRun& qr, const Geom& g0, Stats& st, bool have_env) {
+    int r;
+    Geom g = g0;
+    g.excl_b = (qr.eb >= 0 && qr.ee > qr.eb) ? qr.eb : -1;
+    g.excl_e = (qr.eb >= 0 && qr.ee > qr.eb) ? qr.ee : -1;
+    const HostQuery& hq = *qr.hq;
+    QueryDev qd;
+    if ((r = upload_query(c, hq, "query", &qd))) return r;
+    unsigned long long* cnt;
+    if ((r = bufT(c, "counters", C_N, &cnt))) return r;
+    FSM_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, c->stream));
+    const long long cap = g.tsn;
+    unsigned long long h[C_N] = {0};
+    fsmeld_counters out{};
+    out.m_k = g.m_k;
+    out.segments = g.forsize;
+    out.tail = g.tsn % g.kml;
+
+    if (qr.mode == 2) {  // exact: every valid window through the DP
+        long long *oi;
+        double* od;
+        if ((r = bufT(c, "outi", (size_t)cap, &oi))) return r;
+        if ((r = bufT(c, "outd", (size_t)cap, &od))) return r;
+        qd.cutoff = qr.cutoff;
+        DpJob dj{};
+        dj.q = qd; dj.target = c->d_target; dj.MU = st.MU; dj.SIG = st.SIG;
+        dj.list = nullptr; dj.n_windows = g.tsn; dj.mode = 0; dj.cutoff = qr.cutoff;
+        dj.out_idx = oi; dj.out_dist = od; dj.n_out = cnt + C_OUT; dj.n_cells = cnt + C_CELLS; dj.out_cap = cap; dj.n_valid = cnt + C_VALID;
+        if ((r = run_dp(c, g, dj, g.tsn))) return r;
+        FSM_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+        FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        const long long nout = (long long)h[C_OUT];
+        if ((r = sort_pairs_i64(c, oi, od, nout))) return r;
+        const long long ncopy = std::min<long long>(nout, qr.cap);
+        if (ncopy > 0) {
+            FSM_CUDA_TRY(cudaMemcpyAsync(qr.out_idx, oi, sizeof(long long) * ncopy, cudaMemcpyDeviceToHost, c->stream));
+            if (qr.out_dist) FSM_CUDA_TRY(cudaMemcpyAsync(qr.out_dist, od, sizeof(double) * ncopy, cudaMemcpyDeviceToHost, c->stream));
+        }
+        FSM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        out.valid = (long long)h[C_VALID];
+        out.invalid = g.tsn - out.valid;
+        out.after_lb = out.after_glb = out.exact_evals = out.valid;
+        out.matches = nout;
+        out.dp_cells = (long long)h[C_CELLS];
+        out.threshold = qr.cutoff;
+        if (qr.out_count) *qr.out_count = nout;
+        if (qr.cnt) *qr.cnt = out;
+        return FSMELD_OK;
+    }
+
+    // thresholds
+    double* thr;
+    if ((r = bufT(c, "thr", (size_t)2 * g.S, &thr))) return r;
+    std::vector<ThrJob> jobs(1);
+    jobs[0].q = qd; jobs[0].Un = st.Un; jobs[0].Ln = st.Ln; jobs[0].thr = thr;
+    if ((r = run_thr(c, g, jobs))) return r;
+    (void)have_env;
+
+    long long* segc = nullptr;
+    if ((r = bufT(c, "segc", (size_t)3 * g.S, &segc))) return r;
+
+    if (qr.mode == 0) {  // search
+        long long* surv;
+        if ((r = bufT(c, "surv", (size_t)cap, &surv))) return r;
+        qd.cutoff = qr.cutoff;
+        LbJob lj{};
+        lj.q = qd; lj.Un = st.Un; lj.Ln = st.Ln; lj.thr = thr; lj.SIG = st.SIG;
+        lj.zout = nullptr; lj.surv = surv; lj.surv_cap = cap; lj.nsurv = cnt + C_SURV;
+        lj.nvalid = cnt + C_VALID; lj.segc = segc;
+        if ((r = run_lbip(c, g, lj))) return r;
+        return search_tail(c, g, qd, st, surv, cnt, cap, segc, qr);
+    }
+
+    // cutoff (top-k)
+    double* z;
+    if ((r = bufT(c, "zbuf", (size_t)g.S * g.kml, &z))) return r;
+    LbJob lj{};
+    lj.q = qd; lj.Un = st.Un; lj.Ln = st.Ln; lj.thr = thr; lj.SIG = st.SIG;
+    lj.zout = z; lj.surv = nullptr; lj.nsurv = cnt + C_SURV; lj.nvalid = cnt + C_VALID; lj.segc = nullptr;
+    if ((r = run_lbip(c, g, lj))) return r;
+    return cutoff_tail(c, g, qd, st, z, cnt, qr);
+}
+
 // ------------------------------------------------ tensor-core LB_IP (groups)
 
 // src/q_to_h.cpp:11-64 (lower) / 84-134 (upper), the penalties of k_lbip
@@ -1007,11 +1022,12 @@ static int gemm_thresholds(fsmeld_ctx* c, const Geom& g, const Stats& st, const 
     return FSMELD_OK;
 }
 
-// Search for queries of equal (m, w) and metric with LB_IP as one
-// tensor-core product per chunk of up to 128 queries (k_lbgemm), then GLB and
-// the exact DP per query as in run_query.  Match sets are those of the
-// per-query path (every bound is a lower bound); the LB_IP survivor counters
-// differ (one shared threshold pair instead of one per segment and query).
+// Searches (top-k queries) of equal (m, w), mode and metric with LB_IP as one
+// tensor-core product per chunk of up to 128 (16) queries (k_lbgemm), then
+// per query GLB and the exact DP (the top-k selection) as in run_query.
+// Match sets and rankings are those of the per-query path (every bound is a
+// lower bound); the LB_IP survivor counters differ (one shared threshold
+// pair instead of one per segment and query).
 static int run_search_gemm(fsmeld_ctx* c, const Geom& g0, Stats& st, const std::vector<const QueryRun*>& qs,
                            std::vector<int>* qstatus, double* zout_dev = nullptr, double* diag = nullptr) {
     int r;
@@ -1023,8 +1039,9 @@ static int run_search_gemm(fsmeld_ctx* c, const Geom& g0, Stats& st, const std::
     const int kpad = kchunks * kLbGemmKChunk;
     const long long cap = g0.tsn;
     const long long words = (g0.tsn + 31) / 32 + 1;
-    for (size_t q0 = 0; q0 < qs.size(); q0 += 128) {
-        const int nq = (int)std::min<size_t>(128, qs.size() - q0);
+    for (size_t q0 = 0; q0 < qs.size(); q0 += (qs[0]->mode == 1 ? 16 : 128)) {
+        const bool topk = qs[0]->mode == 1;
+        const int nq = (int)std::min<size_t>(topk ? 16 : 128, qs.size() - q0);
         const int NQ = nq <= 16 ? 16 : nq <= 32 ? 32 : nq <= 64 ? 64 : 128;
         // B operand and margins
         std::vector<uint16_t> B((size_t)kchunks * 6 * NQ * kLbGemmKChunk, 0);
@@ -1062,7 +1079,7 @@ static int run_search_gemm(fsmeld_ctx* c, const Geom& g0, Stats& st, const std::
                 // split's residual and a relative 2^-40 for these host sums
                 marg[2 * i + side] = (R + 4.0 * nadd * std::ldexp(S, -23)) * (1.0 + std::ldexp(1.0, -40)) + 1e-300;
             }
-            cut[i] = qr.cutoff;
+            cut[i] = topk ? DBL_MAX : qr.cutoff;
             met[i] = hq.metric;
             const bool ex = qr.eb >= 0 && qr.ee > qr.eb;
             eb[i] = ex ? qr.eb : -1;
@@ -1099,8 +1116,10 @@ static int run_search_gemm(fsmeld_ctx* c, const Geom& g0, Stats& st, const std::
         gj.B = (const uint4*)dB; gj.m = m; gj.nq = nq; gj.kchunks = kchunks;
         gj.margin_l = dM; gj.margin_u = dM + nq; gj.metric = dMet; gj.cutoff = dC;
         gj.excl_b = dE; gj.excl_e = dE + nq;
-        gj.zout = zout_dev; gj.zstride = g0.S * g0.kml;
-        gj.bits = dbits; gj.bit_words = words;
+        double* zq = zout_dev;
+        if (topk && !zq && (r = bufT(c, "gemmZ", (size_t)nq * g0.S * g0.kml, &zq))) return r;
+        gj.zout = zq; gj.zstride = g0.S * g0.kml;
+        gj.bits = topk ? nullptr : dbits; gj.bit_words = words;
         gj.nsurv = dcnt; gj.nvalid = dcnt + nq; gj.err = (unsigned*)(dcnt + 2 * nq);
         const void* kf = lbgemm_kernel(NQ);
         const size_t smem = lbgemm_smem_bytes(NQ, m);
@@ -1138,6 +1157,16 @@ static int run_search_gemm(fsmeld_ctx* c, const Geom& g0, Stats& st, const std::
             if ((r = bufT(c, "counters", C_N, &cnt))) return r;
             FSM_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, c->stream));
             FSM_CUDA_TRY(cudaMemcpyAsync(cnt + C_VALID, dcnt + nq + i, 8, cudaMemcpyDeviceToDevice, c->stream));
+            if (topk) {
+                if ((long long)hc[nq + i] < qr.k) {
+                    (*qstatus)[q0 + i] = fail(FSMELD_E_FEWER_K, "Fewer valid, non-excluded candidates than requested k.");
+                    continue;
+                }
+                const int q = cutoff_tail(c, g, qd, st, zq + (size_t)i * g0.S * g0.kml, cnt, qr);
+                (*qstatus)[q0 + i] = q;
+                if (q == FSMELD_E_CUDA) return q;
+                continue;
+            }
             long long* surv;
             if ((r = bufT(c, "surv", (size_t)cap, &surv))) return r;
             prof_begin(c, ST_LBIP);
@@ -1188,19 +1217,20 @@ static int get_worker(fsmeld_ctx* c, int i, fsmeld_ctx** out) {
 }
 
 
-// Searches of one (m, w) group (order[gi..gj)) through the tensor-core LB_IP
-// when it is selected: one product per metric with at least two searches.
-// Marks the queries it ran in `done`.
+// Searches and top-k queries of one (m, w) group (order[gi..gj)) through the
+// tensor-core LB_IP when it is selected: one product per mode and metric with
+// at least two queries.  Marks the queries it ran in `done`.
 static int group_gemm(fsmeld_ctx* c, const Geom& g, Stats& st, std::vector<QueryRun>& runs,
                       const std::vector<size_t>& order, size_t gi, size_t gj, std::vector<int>* status,
                       std::vector<char>* done) {
     if (c->lb_form == 1) return FSMELD_OK;
+    for (int mode = 0; mode <= 1; ++mode)
     for (int metric = DTW; metric <= MSM; ++metric) {
         std::vector<const QueryRun*> qs;
         std::vector<size_t> idx;
         for (size_t k = gi; k < gj; ++k) {
             const QueryRun& qr = runs[order[k]];
-            if (qr.mode == 0 && qr.hq->metric == metric) { qs.push_back(&qr); idx.push_back(k); }
+            if (qr.mode == mode && qr.hq->metric == metric) { qs.push_back(&qr); idx.push_back(k); }
         }
         if (qs.size() < 2) continue;
         if (c->lb_form == 0 && tuned(c, 1, metric, g.m_k, (int)qs.size()) != 2) continue;

@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_lbgemm(Geom g, GemmJob job) {
                 const unsigned bk = __ballot_sync(0xffffffffu, keep);
                 if (lane == 0 && q < job.nq) {
                     if (bv) atomicAdd(&s_valid[i], __popc(bv));
-                    if (bk) {
+                    if (bk && job.bits) {
                         atomicAdd(&s_cnt[i], __popc(bk));
                         unsigned* bq = job.bits + (size_t)q * job.bit_words;
                         const long long w0 = p0 >> 5;  // floor for negative p0 (short targets' tail)

@@ -130,14 +130,15 @@ int fsmeld_set_concurrency(fsmeld_ctx* ctx, int queries);
 int fsmeld_set_normalization(fsmeld_ctx* ctx, int mode);
 int fsmeld_normalization(const fsmeld_ctx* ctx);
 
-/* LB_IP form of batched searches (fsmeld_batch, mode 0) whose queries share
- * (m, w) and metric (no reference counterpart; the reference computes LB_IP
+/* LB_IP form of batched searches and top-k queries (fsmeld_batch, modes 0
+ * and 1) whose queries share (m, w) and metric (no reference counterpart; the reference computes LB_IP
  * per query with FFTs, src/sip.cpp:16-52).  FSMELD_LB_FFT: per query and
  * segment, the reference's threshold selection and an FP64 FFT.
  * FSMELD_LB_GEMM: one threshold pair for the group and the sliding inner
  * products of all its queries as one tensor-core product (BF16x3 split, FP32
  * accumulation, each bound lowered by its rounding-error margin).  Match
- * sets are the same either way; the LB_IP survivor counters differ.
+ * sets and rankings are the same either way; the LB_IP survivor counters
+ * differ.
  * FSMELD_LB_AUTO (default): the tuner's choice for the group's shape. */
 #define FSMELD_LB_AUTO 0
 #define FSMELD_LB_FFT 1

@@ -101,3 +101,25 @@ def test_config2_vs_reference(api, pins):
             below = np.nextafter(cut, 0.0)
             bidx, bc = e.search(q, m, below, metric, w, arg)
             assert len(bidx) == mp["matches_below"] < p["k"], metric
+
+
+@pytest.mark.parametrize("k", [10, 100])
+def test_config4_shape_rankings_vs_oracle(api, oracle, k):
+    # the top-k configuration's shape (DTW, m=512, w=26, walk with noise
+    # bursts) on a 2^18-point target: GPU rankings (distance, index, ties
+    # included) equal the oracle's, through both LB_IP forms of a batch
+    from fsmeld_b200.synth import query_from, walk_with_bursts
+
+    m, w = 512, 26
+    t = walk_with_bursts(1 << 18, m, seed=44)
+    rng = np.random.default_rng(4404)
+    qs = [query_from(t, m, rng)[0] for _ in range(2)]
+    want = [oracle.cutoff(t, q, m, k, "dtw", w, 0.0) for q in qs]
+    with api.Engine(t) as e:
+        for form in ("fft", "gemm"):
+            e.set_lb_form(form)
+            got = e.batch("cutoff", [dict(query=q, m=m, metric="dtw", w=w, arg=0.0, k=k) for q in qs])
+            for g_, (oidx, odist, _) in zip(got, want):
+                assert g_["status"] == 0
+                assert list(g_["idx"]) == list(oidx), form
+                assert _hex(g_["dist"]) == _hex(odist), form

@@ -106,3 +106,23 @@ def test_gemm_batched_search_equals_oracle(oracle, target):
         assert list(g_["idx"]) == list(oidx) == list(f_["idx"]), d["metric"]
         assert g_["counters"]["valid"] == oc["valid"] == f_["counters"]["valid"]
         assert g_["counters"]["matches"] == oc["matches"]
+
+
+def test_gemm_batched_topk_equals_oracle(oracle, target):
+    from fsmeld_b200 import api
+
+    t, m, w = target
+    rng = np.random.default_rng(811)
+    batch = []
+    for metric, arg in [("dtw", 0.0), ("msm", 0.5), ("lcss", 0.25)]:
+        for _ in range(3):
+            q, _ = query_from(t, m, rng)
+            batch.append(dict(query=q, m=m, metric=metric, w=w, arg=arg, k=7))
+    with api.Engine(t) as e:
+        e.set_lb_form("gemm")
+        got = e.batch("cutoff", batch)
+    for d, g_ in zip(batch, got):
+        oidx, odist, _ = oracle.cutoff(t, d["query"], m, 7, d["metric"], w, d["arg"])
+        assert g_["status"] == 0
+        assert list(g_["idx"]) == list(oidx), d["metric"]
+        assert np.array_equal(np.asarray(g_["dist"]).view(np.int64), np.asarray(odist).view(np.int64))
