@@ -232,8 +232,8 @@ struct fsmeld_ctx {
     struct ProfRec { int stage; cudaEvent_t a, b; };
     std::vector<ProfRec> pending;
     std::vector<cudaEvent_t> pool;
-    double stage_ms[8] = {0};
-    long long stage_n[8] = {0};
+    double stage_ms[16] = {0};
+    long long stage_n[16] = {0};
 };
 
 namespace fsm {
@@ -276,9 +276,10 @@ static int allow_smem(fsmeld_ctx* c, K kernel, size_t bytes) {
     return FSMELD_OK;
 }
 
-enum Stage { ST_STATS, ST_ENV, ST_THR, ST_LBIP, ST_GLB1, ST_GLB2, ST_DP, ST_SELECT, ST_N };
+enum Stage { ST_STATS, ST_ENV, ST_THR, ST_LBIP, ST_GLB1, ST_GLB2, ST_DP, ST_SELECT, ST_FWD, ST_DPW, ST_GEMM, ST_N };
 static const char* kStageNames[ST_N] = {"k_mvmean", "k_envelope", "k_threshold", "k_lbip",
-                                        "k_glb_tq", "k_glb_qt", "k_dp", "k_select"};
+                                        "k_glb_tq", "k_glb_qt", "k_dp", "k_select",
+                                        "k_fwd_env", "k_dpw", "k_lbgemm"};
 
 static cudaEvent_t prof_event(fsmeld_ctx* c) {
     if (!c->pool.empty()) { cudaEvent_t e = c->pool.back(); c->pool.pop_back(); return e; }
@@ -430,10 +431,17 @@ static int run_env(fsmeld_ctx* c, const Geom& g, int w, Stats* st, const std::st
     if ((r = bufT(c, "ln" + tag, (size_t)g.S * g.m_k, &st->Ln))) return r;
     if ((r = bufT(c, "lraw" + tag, (size_t)g.n, &st->Lraw))) return r;
     if ((r = bufT(c, "uraw" + tag, (size_t)g.n, &st->Uraw))) return r;
-    prof_begin(c, ST_ENV);
-    k_fwd_env<<<(unsigned)std::min<long long>((g.n + 255) / 256, (long long)c->sm_count * 32), 256, 0, c->stream>>>(
-        c->d_target, g.n, w, st->Lraw, st->Uraw);
-    LAUNCH_CHECK(c);
+    {
+        const size_t fsm = fwd_env_smem_bytes(w);
+        if ((r = allow_smem(c, k_fwd_env, fsm))) return r;
+        int per_sm = 0;
+        FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fwd_env, kFwdThreads, fsm));
+        const unsigned fgrid = (unsigned)std::max<long long>(
+            1, std::min<long long>((g.n + kFwdTile - 1) / kFwdTile, (long long)std::max(1, per_sm) * c->sm_count));
+        prof_begin(c, ST_FWD);
+        k_fwd_env<<<fgrid, kFwdThreads, fsm, c->stream>>>(c->d_target, g.n, w, st->Lraw, st->Uraw);
+        LAUNCH_CHECK(c);
+    }
     const int mk = g.m_k;
     if (mk <= 1024) return launch_env<128, 8>(c, g, w, st);
     if (mk <= 2048) return launch_env<256, 8>(c, g, w, st);
@@ -635,7 +643,7 @@ static int run_dp(fsmeld_ctx* c, const Geom& g, DpJob job, long long expected) {
         FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wk, kDpwThreads, wsm));
         const long long want = (expected + kDpwThreads / 32 - 1) / (kDpwThreads / 32);
         grid = (unsigned)std::max<long long>(1, std::min<long long>(want, (long long)std::max(1, per_sm) * c->sm_count));
-        prof_begin(c, ST_DP);
+        prof_begin(c, ST_DPW);
         Geom ga = g;
         void* args[] = {&ga, &job};
         const cudaError_t le = cudaLaunchKernel(wk, dim3(grid), dim3(kDpwThreads), args, wsm, c->stream);
@@ -1132,7 +1140,7 @@ static int run_search_gemm(fsmeld_ctx* c, const Geom& g0, Stats& st, const std::
         const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(items, (long long)per_sm * c->sm_count));
         Geom ga = g0;
         void* args[] = {&ga, &gj};
-        prof_begin(c, ST_LBIP);
+        prof_begin(c, ST_GEMM);
         const cudaError_t le = cudaLaunchKernel(kf, dim3(grid), dim3(kLbGemmThreads), args, smem, c->stream);
         if (le != cudaSuccess) return cuda_fail(le, "k_lbgemm launch", __FILE__, __LINE__);
         LAUNCH_CHECK(c);

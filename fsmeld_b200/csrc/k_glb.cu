@@ -199,22 +199,70 @@ __global__ void __launch_bounds__(256, 4) k_glb_tq(Geom g, GlbJob job) {
 }
 
 // Forward windows of the raw target: lo/up[p] = min/max(t[p .. min(n-1, p+w)])
-// (NaN ignored; only windows inside valid candidate windows are ever read).
-__global__ void __launch_bounds__(256) k_fwd_env(const double* __restrict__ t, long long n, int w,
-                                                 double* __restrict__ lo, double* __restrict__ up) {
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n;
-         p += (long long)gridDim.x * blockDim.x) {
-        const long long b = p + w > n - 1 ? n - 1 : p + w;
-        double mn = t[p], mx = t[p];
-        for (long long i = p + 1; i <= b; ++i) {
-            const double v = t[i];
-            mn = fmin(mn, v);
-            mx = fmax(mx, v);
+// with fmin/fmax (NaN ignored unless the whole window is NaN; only windows
+// inside valid candidate windows, which hold no NaN, are ever read).
+//
+// Doubling in shared memory: after pass k, M[i] = min(t[i .. i + 2^k - 1]);
+// a window of length L = w+1 is the union of the two length-2^K runs at its
+// ends (2^K <= L < 2^(K+1)), min(M[p], M[p + L - 2^K]) -- the same set, so
+// the same value as a direct scan.  log2(L) passes of one min per element
+// replace the L reads per output of a direct scan, so the cost no longer
+// grows with the radius.  A CTA produces kFwdTile outputs per tile from the
+// tile plus its w-point halo, ping-ponging between two shared buffers.
+__global__ void __launch_bounds__(kFwdThreads) k_fwd_env(const double* __restrict__ t, long long n, int w,
+                                                        double* __restrict__ lo, double* __restrict__ up) {
+    extern __shared__ double fw_smem[];
+    const int ext = kFwdTile + w;  // tile plus halo
+    double* An = fw_smem;
+    double* Ax = An + ext;
+    double* Bn = Ax + ext;
+    double* Bx = Bn + ext;
+    const int L = w + 1;
+    int K = 0;
+    while ((2 << K) <= L) ++K;  // 2^K <= L < 2^(K+1)
+    const int off = L - (1 << K);
+    for (long long p0 = (long long)blockIdx.x * kFwdTile; p0 < n; p0 += (long long)gridDim.x * kFwdTile) {
+        const int cnt = (int)((n - p0) < ext ? (n - p0) : ext);
+        for (int i = threadIdx.x; i < ext; i += kFwdThreads) {
+            const double v = i < cnt ? t[p0 + i] : NAN;
+            An[i] = v;
+            Ax[i] = v;
         }
-        lo[p] = mn;
-        up[p] = mx;
+        __syncthreads();
+        for (int k = 0; k < K; ++k) {
+            const int s = 1 << k;
+            for (int i = threadIdx.x; i < ext; i += kFwdThreads) {
+                const bool in = i + s < ext;
+                Bn[i] = in ? fmin(An[i], An[i + s]) : An[i];
+                Bx[i] = in ? fmax(Ax[i], Ax[i + s]) : Ax[i];
+            }
+            __syncthreads();
+            double* tn = An; An = Bn; Bn = tn;
+            double* tx = Ax; Ax = Bx; Bx = tx;
+        }
+        for (int i = threadIdx.x; i < kFwdTile; i += kFwdThreads) {
+            const long long p = p0 + i;
+            if (p >= n) break;
+            double mn, mx;
+            if (p + w <= n - 1) {
+                mn = fmin(An[i], An[i + off]);
+                mx = fmax(Ax[i], Ax[i + off]);
+            } else {  // the last w points: the window is clipped at the end of the target
+                mn = t[p];
+                mx = t[p];
+                for (long long j = p + 1; j < n; ++j) {
+                    mn = fmin(mn, t[j]);
+                    mx = fmax(mx, t[j]);
+                }
+            }
+            lo[p] = mn;
+            up[p] = mx;
+        }
+        __syncthreads();
     }
 }
+
+size_t fwd_env_smem_bytes(int w) { return sizeof(double) * 4 * (size_t)(kFwdTile + w); }
 
 // one lane per T->Q survivor: Q->T terms added in the reference's order
 template <int METRIC>

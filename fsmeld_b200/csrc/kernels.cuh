@@ -125,8 +125,13 @@ template <int METRIC>
 __global__ void k_glb_tq(Geom g, GlbJob job);
 template <int METRIC>
 __global__ void k_glb_qt(Geom g, GlbJob job);
+// forward windows min/max(t[p .. p+w]) by doubling in shared memory, kFwdTile
+// outputs per CTA and tile
+constexpr int kFwdThreads = 256;
+constexpr int kFwdTile = 2048;
 __global__ void k_fwd_env(const double* __restrict__ t, long long n, int w, double* __restrict__ lo,
                           double* __restrict__ up);
+size_t fwd_env_smem_bytes(int w);
 template <int METRIC, bool GW>
 __global__ void k_dp(Geom g, DpJob job);
 // the DP kernel for a metric, with its band in shared memory or in job.gwork
