@@ -443,9 +443,9 @@ static int run_env(fsmeld_ctx* c, const Geom& g, int w, Stats* st, const std::st
         LAUNCH_CHECK(c);
     }
     const int mk = g.m_k;
-    if (mk <= 1024) return launch_env<128, 8>(c, g, w, st);
-    if (mk <= 2048) return launch_env<256, 8>(c, g, w, st);
-    if (mk <= 4096) return launch_env<512, 8>(c, g, w, st);
+    if (mk <= 1024) return launch_env<256, 4>(c, g, w, st);
+    if (mk <= 2048) return launch_env<512, 4>(c, g, w, st);
+    if (mk <= 4096) return launch_env<1024, 4>(c, g, w, st);
     if (mk <= 8192) return launch_env<1024, 8>(c, g, w, st);
     if (mk <= 16384) return launch_env<1024, 16>(c, g, w, st);
     return fail(FSMELD_E_UNSUPPORTED, "macro segments longer than 16384 points are not supported");

@@ -6,15 +6,20 @@
 // The reference uses monotone deques.  Their outputs have a closed form that
 // this kernel computes in parallel:
 //  * with no NaN in the window: the window minimum (maximum); among equal
-//    values the most recent one (the deque pops older elements that compare
-//    >= / <= the newcomer), which only matters for the sign of a zero;
+//    values the deque keeps the most recent one, which only matters for the
+//    sign of a zero (window means and sigmas are never -0; a target's -0 and
+//    +0 give the same U_normal / L_normal comparisons and penalties);
 //  * with a NaN in the window: a NaN blocks every pop behind it, so the
 //    front is the extremum of the points before the first NaN, or NaN when
 //    the window starts with NaN.
-// NaN-free windows use van Herk / Gil-Werman: block-local prefix and suffix
-// extrema (blocks of the window length B) computed by a block-segmented scan,
-// then one combine per output.  Windows that contain a NaN (detected with a
-// NaN prefix count) are evaluated directly from their start.
+// NaN-free windows by doubling: after pass k, M[i] = min(x[i .. i+2^k-1]);
+// a window [a, b] of length L with 2^k <= L < 2^(k+1) is the union of the
+// runs of length 2^k at its two ends, min(M[a], M[b-2^k+1]), so each output
+// is taken right after the pass of its own level (full windows, and the
+// shorter windows at the segment's edges alike).  Every pass is one min and
+// one max per element with a block barrier, no scans.  Windows that contain
+// a NaN (detected with a NaN prefix count) are evaluated directly from their
+// start.
 #include <cub/block/block_scan.cuh>
 
 #include "common.cuh"
@@ -23,32 +28,6 @@
 namespace fsm {
 
 namespace {
-
-struct MMCarry {
-    double mn, mx;
-    int fl;  // bit 0: chunk contains a block start; bit 1: chunk non-empty
-};
-
-// combine(a = earlier in scan order, b = later); FWD scans run old -> new,
-// REV scans run new -> old; ties keep the newer element.
-template <bool REV>
-struct MMComb {
-    __device__ MMCarry operator()(const MMCarry& a, const MMCarry& b) const {
-        MMCarry r;
-        r.fl = a.fl | b.fl;
-        if (b.fl & 1) { r.mn = b.mn; r.mx = b.mx; return r; }
-        if (!(b.fl & 2)) { r.mn = a.mn; r.mx = a.mx; return r; }
-        if (!(a.fl & 2)) { r.mn = b.mn; r.mx = b.mx; return r; }
-        if (!REV) {  // a older, b newer
-            r.mn = (b.mn <= a.mn) ? b.mn : a.mn;
-            r.mx = (b.mx >= a.mx) ? b.mx : a.mx;
-        } else {     // a newer, b older
-            r.mn = (a.mn <= b.mn) ? a.mn : b.mn;
-            r.mx = (a.mx >= b.mx) ? a.mx : b.mx;
-        }
-        return r;
-    }
-};
 
 // Padded index of the per-segment arrays: one spare slot after every 8
 // elements, so the blocked walks of the scans (thread t on elements
@@ -59,58 +38,8 @@ __host__ __device__ inline int env_pad_len(int n) { return n + (n >> 3) + 2; }
 
 template <int T>
 struct EnvTemp {
-    union {
-        typename cub::BlockScan<MMCarry, T>::TempStorage mm;
-        typename cub::BlockScan<int, T>::TempStorage ic;
-    };
+    typename cub::BlockScan<int, T>::TempStorage ic;
 };
-
-// Block-segmented inclusive min/max scan, in place, blocks [kB, (k+1)B).
-// REV = false: prefix within blocks; REV = true: suffix within blocks.
-template <int T, bool REV>
-__device__ void seg_scan(double* mn, double* mx, int n, int B, EnvTemp<T>& tmp) {
-    const int t = threadIdx.x;
-    const int c = (n + T - 1) / T;
-    const int lo = t * c, hi = min(n, lo + c);
-    double rmn = 0.0, rmx = 0.0;
-    int fl = 0, first_start = hi;
-    for (int u = lo; u < hi; ++u) {
-        const int i = REV ? n - 1 - u : u;
-        const bool start = REV ? (u == 0 || (i % B) == B - 1) : ((i % B) == 0);
-        const double xmn = mn[px(i)], xmx = mx[px(i)];
-        if (start || !(fl & 2)) {
-            rmn = xmn;
-            rmx = xmx;
-            if (start && !(fl & 1)) first_start = u;
-            fl |= 2 | (start ? 1 : 0);
-        } else if (!REV) {
-            rmn = (xmn <= rmn) ? xmn : rmn;
-            rmx = (xmx >= rmx) ? xmx : rmx;
-        } else {
-            rmn = (rmn <= xmn) ? rmn : xmn;
-            rmx = (rmx >= xmx) ? rmx : xmx;
-        }
-        mn[px(i)] = rmn;
-        mx[px(i)] = rmx;
-    }
-    MMCarry mine{rmn, rmx, fl}, cin;
-    cub::BlockScan<MMCarry, T>(tmp.mm).ExclusiveScan(mine, cin, MMComb<REV>());
-    __syncthreads();
-    if (t > 0 && (cin.fl & 2)) {
-        const int e = min(hi, first_start);
-        for (int u = lo; u < e; ++u) {
-            const int i = REV ? n - 1 - u : u;
-            if (!REV) {
-                mn[px(i)] = (mn[px(i)] <= cin.mn) ? mn[px(i)] : cin.mn;
-                mx[px(i)] = (mx[px(i)] >= cin.mx) ? mx[px(i)] : cin.mx;
-            } else {
-                mn[px(i)] = (cin.mn <= mn[px(i)]) ? cin.mn : mn[px(i)];
-                mx[px(i)] = (cin.mx >= mx[px(i)]) ? cin.mx : mx[px(i)];
-            }
-        }
-    }
-    __syncthreads();
-}
 
 struct EnvWork {
     double *raw, *Pmn, *Pmx, *Smn, *Smx;
@@ -118,18 +47,20 @@ struct EnvWork {
 };
 
 // Sliding min/max of src[0..n) for nout windows; CENTRED selects
-// [o-w, o+w] (lemire) versus the trailing [o-m+1, o] (min_max_window).
+// [o-w, o+w] (lemire) versus the trailing [o-m+1, o] (min_max_window), both
+// clipped to [0, n-1].  Work arrays: raw copy, two ping-pong pairs (Pmn/Pmx,
+// Smn/Smx) for the doubling passes, NaN prefix counts.
 template <int T, int OPT, bool CENTRED>
 __device__ void minmax_phase(const double* __restrict__ src, int n, int par, int nout,
                              const EnvWork& wk, EnvTemp<T>& tmp, double (&omn)[OPT],
                              double (&omx)[OPT]) {
     const int t = threadIdx.x;
-    const int B = CENTRED ? 2 * par + 1 : par;
     int local_nan = 0;
     for (int i = t; i < n; i += T) {
         const double v = src[i];
         wk.raw[px(i)] = v;
-        wk.Pmn[px(i)] = v; wk.Pmx[px(i)] = v; wk.Smn[px(i)] = v; wk.Smx[px(i)] = v;
+        wk.Pmn[px(i)] = v;
+        wk.Pmx[px(i)] = v;
         local_nan |= isnan(v) ? 1 : 0;
     }
     const int any_nan = __syncthreads_or(local_nan);
@@ -145,41 +76,71 @@ __device__ void minmax_phase(const double* __restrict__ src, int n, int par, int
             off += isnan(wk.raw[px(i)]) ? 1 : 0;
         }
         if (hi == n && lo < hi) wk.ncnt[px(n)] = off;  // the chunk holding n-1 closes the count
+        __syncthreads();
     }
-    __syncthreads();
-    seg_scan<T, false>(wk.Pmn, wk.Pmx, n, B, tmp);
-    seg_scan<T, true>(wk.Smn, wk.Smx, n, B, tmp);
+    // each output's window [ws, we] (recomputed where needed, to keep the
+    // per-thread state to the outputs themselves)
+    auto window = [&](int o, int& ws, int& we) {
+        if (CENTRED) { ws = max(0, o - par); we = min(n - 1, o + par); }
+        else { ws = max(0, o - par + 1); we = min(o, n - 1); }
+    };
+    auto has_nan = [&](int ws, int we) {
+        return any_nan && (wk.ncnt[px(we + 1)] - wk.ncnt[px(ws)] > 0);
+    };
+#pragma unroll
+    for (int k = 0; k < OPT; ++k) { omn[k] = 0.0; omx[k] = 0.0; }
+    // the deepest level any window needs: the full window length, clipped to n
+    const int maxlen = CENTRED ? min(n, 2 * par + 1) : min(n, par);
+    const int levels = 31 - __clz(max(1, maxlen));
+    double* An = wk.Pmn;
+    double* Ax = wk.Pmx;
+    double* Bn = wk.Smn;
+    double* Bx = wk.Smx;
+    for (int lv = 0; lv <= levels; ++lv) {
+        if (lv > 0) {
+            const int s = 1 << (lv - 1);
+            for (int i = t; i < n; i += T) {
+                const bool in = i + s < n;
+                const double a0 = An[px(i)], x0 = Ax[px(i)];
+                const double a1 = in ? An[px(i + s)] : a0, x1 = in ? Ax[px(i + s)] : x0;
+                Bn[px(i)] = (a1 < a0) ? a1 : a0;
+                Bx[px(i)] = (x1 > x0) ? x1 : x0;
+            }
+            __syncthreads();
+            double* tn = An; An = Bn; Bn = tn;
+            double* tx = Ax; Ax = Bx; Bx = tx;
+        }
+        // outputs whose window length has this level: the two end runs
+#pragma unroll
+        for (int k = 0; k < OPT; ++k) {
+            const int o = t + k * T;
+            if (o >= nout) continue;
+            int ws, we;
+            window(o, ws, we);
+            if (31 - __clz(we - ws + 1) != lv || has_nan(ws, we)) continue;
+            const int b2 = we - (1 << lv) + 1;
+            const double a0 = An[px(ws)], a1 = An[px(b2)];
+            const double x0 = Ax[px(ws)], x1 = Ax[px(b2)];
+            omn[k] = (a1 < a0) ? a1 : a0;
+            omx[k] = (x1 > x0) ? x1 : x0;
+        }
+    }
+    // windows holding a NaN: the deque's front from the window's start
 #pragma unroll
     for (int k = 0; k < OPT; ++k) {
         const int o = t + k * T;
-        double vmn = 0.0, vmx = 0.0;
-        if (o < nout) {
-            int ws, we;
-            if (CENTRED) { ws = max(0, o - par); we = min(n - 1, o + par); }
-            else { ws = max(0, o - par + 1); we = min(o, n - 1); }
-            const bool nanwin = any_nan && (wk.ncnt[px(we + 1)] - wk.ncnt[px(ws)] > 0);
-            if (nanwin) {
-                double a = wk.raw[px(ws)];
-                if (isnan(a)) {
-                    vmn = a; vmx = a;
-                } else {
-                    vmn = a; vmx = a;
-                    for (int i = ws + 1; i <= we; ++i) {
-                        const double v = wk.raw[px(i)];
-                        if (isnan(v)) break;
-                        vmn = (v <= vmn) ? v : vmn;
-                        vmx = (v >= vmx) ? v : vmx;
-                    }
-                }
-            } else if (ws % B == 0) {
-                vmn = wk.Pmn[px(we)]; vmx = wk.Pmx[px(we)];
-            } else if (ws / B == we / B) {
-                vmn = wk.Smn[px(ws)]; vmx = wk.Smx[px(ws)];
-            } else {
-                const double pm = wk.Pmn[px(we)], sm = wk.Smn[px(ws)];
-                const double pxv = wk.Pmx[px(we)], sx = wk.Smx[px(ws)];
-                vmn = (pm <= sm) ? pm : sm;
-                vmx = (pxv >= sx) ? pxv : sx;
+        if (!any_nan || o >= nout) continue;
+        int ws, we;
+        window(o, ws, we);
+        if (!has_nan(ws, we)) continue;
+        double a = wk.raw[px(ws)];
+        double vmn = a, vmx = a;
+        if (!isnan(a)) {
+            for (int i = ws + 1; i <= we; ++i) {
+                const double v = wk.raw[px(i)];
+                if (isnan(v)) break;
+                vmn = (v <= vmn) ? v : vmn;
+                vmx = (v >= vmx) ? v : vmx;
             }
         }
         omn[k] = vmn;
@@ -235,9 +196,9 @@ size_t envelope_work_bytes(int m_k) { return (size_t)env_pad_len(m_k) * (5 * siz
                                                        Geom, int, double*, double*, double*, long long); \
     template __global__ void k_envelope<T, OPT, true>(const double*, const double*, const double*,   \
                                                       Geom, int, double*, double*, double*, long long);
-FSM_ENV_INST(128, 8)
-FSM_ENV_INST(256, 8)
-FSM_ENV_INST(512, 8)
+FSM_ENV_INST(256, 4)
+FSM_ENV_INST(512, 4)
+FSM_ENV_INST(1024, 4)
 FSM_ENV_INST(1024, 8)
 FSM_ENV_INST(1024, 16)
 
