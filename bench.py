@@ -208,6 +208,29 @@ def roofline_hbm(stages, geom, peaks):
             else "fallback 6.65 TB/s"}
 
 
+def stage_rooflines(stages, geom, n, peaks):
+    """HBM fraction of every memory-bound stage, from its algorithmic bytes
+    per launch and its average CUDA-event launch time:
+      k_mvmean   8 B per segment point read (halo included) + 16 B per window
+      k_envelope 8 B per segment point + 16 B per window read, 16 B per point written
+      k_fwd_env  8 B per target point read, 16 B written
+      k_seed / k_lb_filter (k_select): 8 B per window (top-k only)"""
+    S, m_k, kml = geom["S"], geom["m_k"], geom["kml"]
+    per_launch = {"k_mvmean": 8.0 * S * m_k + 16.0 * S * kml,
+                  "k_envelope": 8.0 * S * m_k + 16.0 * S * kml + 16.0 * S * m_k,
+                  "k_fwd_env": 24.0 * n}
+    out = {}
+    for k, b in per_launch.items():
+        if k not in stages or stages[k][1] == 0:
+            continue
+        ms, launches = stages[k]
+        avg_s = ms / launches / 1e3
+        gbs = b / avg_s / 1e9
+        out[k] = {"bound": "hbm", "algorithmic_bytes_per_launch": b, "avg_launch_ms": round(avg_s * 1e3, 4),
+                  "achieved_gbs": round(gbs, 1), "frac": round(gbs / peaks["hbm_gbs"], 4)}
+    return out
+
+
 def geometry(n, m):
     sel = 1
     while sel < 8 * m:
@@ -464,6 +487,7 @@ def impl_ours(args):
             "queries_per_s": len(metrics) * world / (t_max_ms / 1e3 / args.steps),
             "roofline": roofline(stages, cells, peaks),
             "roofline_hbm": roofline_hbm(stages, geom, peaks),
+            "stage_rooflines": stage_rooflines(stages, geom, len(target), peaks),
             "dominant_kernel": max(stages.items(), key=lambda kv: kv[1][0])[0],
             "stage_timing": f"{prof_steps} steps, queries one after another, CUDA events around each launch",
             "stage_ms_per_step": {k: round(v[0] / prof_steps, 4) for k, v in stages.items()},
