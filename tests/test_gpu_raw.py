@@ -5,7 +5,7 @@ query (allowed in raw mode only)."""
 import numpy as np
 import pytest
 
-from fsmeld_b200.synth import walk_with_structure
+from fsmeld_b200.synth import query_from, walk_with_structure
 
 pytestmark = pytest.mark.gpu
 
@@ -29,7 +29,7 @@ def test_raw_mode_vs_oracle(raw_oracle):
     o = raw_oracle
     m, w = 64, 5
     t = walk_with_structure(1 << 16, m, seed=515, motifs=20, nan_fraction=2e-3, flat_runs=6, nan_spans=4)
-    q = t[20_000:20_000 + m] + np.random.default_rng(516).normal(0.0, 0.5, m)
+    q, _ = query_from(t, m, np.random.default_rng(516), noise=0.5)
     with api.Engine(t) as e:
         e.set_normalization("raw")
         assert e.normalization == "raw"
