@@ -217,7 +217,7 @@ struct fsmeld_ctx {
     // tuner's choice), 1 the per-query FFT form, 2 the tensor-core product
     int lb_form = 0;
     // tuning table (fsmeld_set_tuning): rules for the automatic choices
-    struct TuneRule { int kind, metric, m_k, lim, choice; };  // kind 0 dp, 1 lb
+    struct TuneRule { int kind, metric, m_k, lim, choice; };  // kind 0 dp, 1 lb (search), 2 lbk (top-k)
     std::vector<TuneRule> tune;
     // normalisation mode (the reference's set_normalization_mode, include/funcs.h:20-28):
     // false z-score (the reference CLI's only mode), true raw
@@ -608,8 +608,8 @@ static int run_glb(fsmeld_ctx* c, const Geom& g, const QueryDev& qd, const Stats
 
 // The tuning table's choice for a shape: the first rule of `kind` for the
 // metric and macro-segment length whose limit is >= v (dp: v = w, choice
-// 1 lane / 2 wave; lb: v = the group's query count as a lower limit, choice
-// 1 fft / 2 gemm).  0 when no rule matches.
+// 1 lane / 2 wave; lb, lbk: v = the group's query count as a lower limit,
+// choice 1 fft / 2 gemm).  0 when no rule matches.
 static int tuned(const fsmeld_ctx* c, int kind, int metric, int m_k, int v) {
     for (const auto& t : c->tune) {
         if (t.kind != kind || t.metric != metric || t.m_k != m_k) continue;
@@ -1036,8 +1036,12 @@ static int gemm_thresholds(fsmeld_ctx* c, const Geom& g, const Stats& st, const 
 // Match sets and rankings are those of the per-query path (every bound is a
 // lower bound); the LB_IP survivor counters differ (one shared threshold
 // pair instead of one per segment and query).
+static int get_worker(fsmeld_ctx* c, int i, fsmeld_ctx** out);
+static void absorb_worker(fsmeld_ctx* c, fsmeld_ctx* wk);
+
 static int run_search_gemm(fsmeld_ctx* c, const Geom& g0, Stats& st, const std::vector<const QueryRun*>& qs,
-                           std::vector<int>* qstatus, double* zout_dev = nullptr, double* diag = nullptr) {
+                           std::vector<int>* qstatus, double* zout_dev = nullptr, double* diag = nullptr,
+                           bool parallel_tails = false) {
     int r;
     const int m = qs[0]->hq->m, w = qs[0]->hq->w, metric = qs[0]->hq->metric;
     GemmChoice th;
@@ -1152,38 +1156,66 @@ static int run_search_gemm(fsmeld_ctx* c, const Geom& g0, Stats& st, const std::
             if (diag) { diag[0] = th.t_l; diag[1] = th.t_u; diag[2] = marg[0]; diag[3] = marg[1]; }
             return FSMELD_OK;
         }
-        // per query: survivor list from its bits, then GLB + DP
-        for (int i = 0; i < nq; ++i) {
+        // per query: survivor list from its bits (top-k: its bounds), then GLB +
+        // DP, on the worker streams of a top-level context (the device work of
+        // one query's tail is independent of the others')
+        auto tail = [&](fsmeld_ctx* x, int i) -> int {
             const QueryRun& qr = *qs[q0 + i];
             Geom g = g0;
             g.excl_b = eb[i];
             g.excl_e = ee[i];
             QueryDev qd;
-            if ((r = upload_query(c, *qr.hq, "query", &qd))) return r;
+            int rr;
+            if ((rr = upload_query(x, *qr.hq, "query", &qd))) return rr;
             qd.cutoff = qr.cutoff;
             unsigned long long* cnt;
-            if ((r = bufT(c, "counters", C_N, &cnt))) return r;
-            FSM_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, c->stream));
-            FSM_CUDA_TRY(cudaMemcpyAsync(cnt + C_VALID, dcnt + nq + i, 8, cudaMemcpyDeviceToDevice, c->stream));
+            if ((rr = bufT(x, "counters", C_N, &cnt))) return rr;
+            FSM_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * C_N, x->stream));
+            FSM_CUDA_TRY(cudaMemcpyAsync(cnt + C_VALID, dcnt + nq + i, 8, cudaMemcpyDeviceToDevice, x->stream));
             if (topk) {
-                if ((long long)hc[nq + i] < qr.k) {
-                    (*qstatus)[q0 + i] = fail(FSMELD_E_FEWER_K, "Fewer valid, non-excluded candidates than requested k.");
-                    continue;
-                }
-                const int q = cutoff_tail(c, g, qd, st, zq + (size_t)i * g0.S * g0.kml, cnt, qr);
-                (*qstatus)[q0 + i] = q;
-                if (q == FSMELD_E_CUDA) return q;
-                continue;
+                if ((long long)hc[nq + i] < qr.k)
+                    return fail(FSMELD_E_FEWER_K, "Fewer valid, non-excluded candidates than requested k.");
+                return cutoff_tail(x, g, qd, st, zq + (size_t)i * g0.S * g0.kml, cnt, qr);
             }
             long long* surv;
-            if ((r = bufT(c, "surv", (size_t)cap, &surv))) return r;
-            prof_begin(c, ST_LBIP);
-            k_bits_to_list<<<(unsigned)std::min<long long>((words + 255) / 256, (long long)c->sm_count * 8), 256, 0,
-                             c->stream>>>(dbits + (size_t)i * words, words, surv, cap, cnt + C_SURV);
-            LAUNCH_CHECK(c);
-            const int q = search_tail(c, g, qd, st, surv, cnt, cap, nullptr, qr);
-            (*qstatus)[q0 + i] = q;
-            if (q == FSMELD_E_CUDA) return q;
+            if ((rr = bufT(x, "surv", (size_t)cap, &surv))) return rr;
+            prof_begin(x, ST_LBIP);
+            k_bits_to_list<<<(unsigned)std::min<long long>((words + 255) / 256, (long long)x->sm_count * 8), 256, 0,
+                             x->stream>>>(dbits + (size_t)i * words, words, surv, cap, cnt + C_SURV);
+            LAUNCH_CHECK(x);
+            return search_tail(x, g, qd, st, surv, cnt, cap, nullptr, qr);
+        };
+        const int conc = parallel_tails ? std::min(std::max(1, c->concurrency), nq) : 1;
+        if (conc <= 1) {
+            for (int i = 0; i < nq; ++i) {
+                const int q = tail(c, i);
+                (*qstatus)[q0 + i] = q;
+                if (q == FSMELD_E_CUDA) return q;
+            }
+        } else {
+            std::vector<fsmeld_ctx*> ws(conc);
+            for (int t = 0; t < conc; ++t)
+                if ((r = get_worker(c, t, &ws[t]))) return r;
+            std::vector<std::string> errs(conc);
+            std::vector<std::thread> th;
+            for (int t = 0; t < conc; ++t) {
+                th.emplace_back([&, t] {
+                    cudaSetDevice(c->device);
+                    for (int i = t; i < nq; i += conc) {
+                        const int q = tail(ws[t], i);
+                        (*qstatus)[q0 + i] = q;
+                        if (q && errs[t].empty()) errs[t] = g_last_error;
+                        if (q == FSMELD_E_CUDA) break;
+                    }
+                });
+            }
+            for (auto& x : th) x.join();
+            for (int t = 0; t < conc; ++t) absorb_worker(c, ws[t]);
+            for (int i = 0; i < nq; ++i)
+                if ((*qstatus)[q0 + i]) {
+                    for (auto& e : errs) if (!e.empty()) { g_last_error = e; break; }
+                    if ((*qstatus)[q0 + i] == FSMELD_E_CUDA) return FSMELD_E_CUDA;
+                }
         }
     }
     (void)w;
@@ -1230,7 +1262,7 @@ static int get_worker(fsmeld_ctx* c, int i, fsmeld_ctx** out) {
 // at least two queries.  Marks the queries it ran in `done`.
 static int group_gemm(fsmeld_ctx* c, const Geom& g, Stats& st, std::vector<QueryRun>& runs,
                       const std::vector<size_t>& order, size_t gi, size_t gj, std::vector<int>* status,
-                      std::vector<char>* done) {
+                      std::vector<char>* done, bool parallel_tails) {
     if (c->lb_form == 1) return FSMELD_OK;
     for (int mode = 0; mode <= 1; ++mode)
     for (int metric = DTW; metric <= MSM; ++metric) {
@@ -1241,9 +1273,9 @@ static int group_gemm(fsmeld_ctx* c, const Geom& g, Stats& st, std::vector<Query
             if (qr.mode == mode && qr.hq->metric == metric) { qs.push_back(&qr); idx.push_back(k); }
         }
         if (qs.size() < 2) continue;
-        if (c->lb_form == 0 && tuned(c, 1, metric, g.m_k, (int)qs.size()) != 2) continue;
+        if (c->lb_form == 0 && tuned(c, mode == 0 ? 1 : 2, metric, g.m_k, (int)qs.size()) != 2) continue;
         std::vector<int> qst(qs.size(), FSMELD_OK);
-        const int r = run_search_gemm(c, g, st, qs, &qst);
+        const int r = run_search_gemm(c, g, st, qs, &qst, nullptr, nullptr, parallel_tails);
         if (r == FSMELD_E_UNSUPPORTED) continue;  // no usable threshold: per-query path
         for (size_t t = 0; t < idx.size(); ++t) {
             (*status)[order[idx[t]]] = r ? r : qst[t];
@@ -1314,7 +1346,7 @@ static int run_tasks_parallel(fsmeld_ctx* c, std::vector<QueryRun>& runs, const 
                     for (size_t k = gi; k < gj; ++k) need_env = need_env || runs[order[k]].mode != 2;
                     if (need_env && (q = run_env(wk, g, w, &st, ""))) { mark(gi, gj, q); gi = gj; continue; }
                     std::vector<char> done(hi, 0);
-                    if ((q = group_gemm(wk, g, st, runs, order, gi, gj, status, &done)) == FSMELD_E_CUDA) {
+                    if ((q = group_gemm(wk, g, st, runs, order, gi, gj, status, &done, false)) == FSMELD_E_CUDA) {
                         mark(gi, gj, q);
                         break;
                     }
@@ -1400,7 +1432,7 @@ int run_batch(fsmeld_ctx* c, std::vector<QueryRun>& runs, std::vector<int>* stat
         }
         // searches through the tensor-core LB_IP (when selected), then the rest
         std::vector<char> done(oj, 0);
-        if ((r = group_gemm(c, g, st, runs, order, oi, oj, status, &done)) == FSMELD_E_CUDA) return r;
+        if ((r = group_gemm(c, g, st, runs, order, oi, oj, status, &done, true)) == FSMELD_E_CUDA) return r;
         std::vector<size_t> rest;
         for (size_t k = oi; k < oj; ++k)
             if (!done[k]) rest.push_back(order[k]);
@@ -1595,7 +1627,7 @@ int fsmeld_set_tuning(fsmeld_ctx* c, const char* table) {
             return fail(FSMELD_E_ARG, "tuning table: a line is not 'kind metric m_k limit choice'");
         }
         fsmeld_ctx::TuneRule t{};
-        t.kind = !strcmp(kind, "dp") ? 0 : !strcmp(kind, "lb") ? 1 : -1;
+        t.kind = !strcmp(kind, "dp") ? 0 : !strcmp(kind, "lb") ? 1 : !strcmp(kind, "lbk") ? 2 : -1;
         t.metric = !strcmp(metric, "dtw") ? DTW : !strcmp(metric, "erp") ? ERP : !strcmp(metric, "edr") ? EDR
                  : !strcmp(metric, "lcss") ? LCSS : !strcmp(metric, "msm") ? MSM : -1;
         t.m_k = mk;

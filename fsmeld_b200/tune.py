@@ -7,10 +7,11 @@ Two choices depend on the shape and are settled by measurement:
   (one warp per candidate, band in registers), per metric, macro-segment
   length m_k and radius w.  Timed as the exact scan (every window through the
   DP, early abandon at the query's rank-20 distance) on a seeded random walk.
-* the LB_IP form of batched searches (`lb` rules): per-query thresholds and
-  FP64 FFTs, or one tensor-core product for the group, per metric, m_k and
-  group size.  Timed as one batched `search` of the group at each query's
-  rank-10 distance.
+* the LB_IP form of batched searches (`lb` rules) and top-k queries (`lbk`):
+  per-query thresholds and FP64 FFTs, or one tensor-core product for the
+  group, per metric, m_k and group size.  Timed as one batched `search` of
+  the group at each query's rank-10 distance, and one batched `cutoff` k=10,
+  on a 2^22-point random walk.
 
 Shapes where the lane DP's band does not fit shared memory need no
 measurement (the wavefront is the only shared-memory form there).  The table
@@ -32,7 +33,7 @@ from fsmeld_b200.synth import query_from, random_walk
 METRIC_ARGS = {"dtw": 0.0, "erp": 0.0, "edr": 0.25, "lcss": 0.25, "msm": 0.5}
 DP_SHAPES = {64: (2, 3, 6, 13, 31), 128: (3, 6, 13, 26, 51), 256: (6, 13, 26, 51, 94),
              512: (13, 26, 51, 94), 1024: (26, 51, 94), 2048: (51, 94)}
-LB_SHAPES = {128: (2, 8, 32), 256: (2, 8, 32), 512: (2, 8, 32)}
+LB_SHAPES = {128: (8, 32), 256: (8, 32), 512: (8, 32)}
 
 
 def macro_length(m):
@@ -82,9 +83,10 @@ def tune_dp(metrics, shapes, log):
     return rules
 
 
-def tune_lb(metrics, shapes, log):
+def tune_lb(metrics, shapes, log, n=1 << 22):
+    """Search groups (at each query's rank-10 distance) and top-k groups (k=10)."""
     rules = []
-    t = random_walk(1 << 20, 9100)
+    t = random_walk(n, 9100)
     for m, qcounts in shapes.items():
         rng = np.random.default_rng(9101 + m)
         w = max(1, m // 20)
@@ -95,16 +97,17 @@ def tune_lb(metrics, shapes, log):
                 for _ in range(max(qcounts)):
                     q, _ = query_from(t, m, rng)
                     _, d, _ = e.cutoff(q, m, 10, metric, w, arg)
-                    qs.append(dict(query=q, m=m, metric=metric, w=w, arg=arg, cutoff=float(d[-1])))
-                for nq in qcounts:
-                    times = {}
-                    for form in ("fft", "gemm"):
-                        e.set_lb_form(form)
-                        times[form] = timed(e, lambda: e.batch("search", qs[:nq]))
-                    choice = min(times, key=times.get)
-                    log(f"lb {metric} m={m} q={nq}: fft {times['fft']:.2f} ms, gemm {times['gemm']:.2f} ms "
-                        f"-> {choice}")
-                    rules.append((metric, macro_length(m), nq, choice, times))
+                    qs.append(dict(query=q, m=m, metric=metric, w=w, arg=arg, cutoff=float(d[-1]), k=10))
+                for kind, mode in (("lb", "search"), ("lbk", "cutoff")):
+                    for nq in qcounts:
+                        times = {}
+                        for form in ("fft", "gemm"):
+                            e.set_lb_form(form)
+                            times[form] = timed(e, lambda: e.batch(mode, qs[:nq]))
+                        choice = min(times, key=times.get)
+                        log(f"{kind} {metric} m={m} q={nq}: fft {times['fft']:.2f} ms, gemm {times['gemm']:.2f} ms "
+                            f"-> {choice}")
+                        rules.append((kind, metric, macro_length(m), nq, choice, times))
     return rules
 
 
@@ -115,9 +118,9 @@ def write_table(path, dp_rules, lb_rules):
         lines.append(f"dp {metric} {mk} {w} {choice}   # lane {times['lane']:.2f} ms, wave {times['wave']:.2f} ms")
     # lb: for each (metric, m_k) the smallest group size from which the product wins at every measured size
     by_shape = {}
-    for metric, mk, nq, choice, times in lb_rules:
-        by_shape.setdefault((metric, mk), []).append((nq, choice, times))
-    for (metric, mk), rows in by_shape.items():
+    for kind, metric, mk, nq, choice, times in lb_rules:
+        by_shape.setdefault((kind, metric, mk), []).append((nq, choice, times))
+    for (kind, metric, mk), rows in by_shape.items():
         rows.sort()
         qmin = None
         for i, (nq, _, _) in enumerate(rows):
@@ -126,9 +129,9 @@ def write_table(path, dp_rules, lb_rules):
                 break
         detail = ", ".join(f"q={nq}: fft {tm['fft']:.1f} / gemm {tm['gemm']:.1f} ms" for nq, _, tm in rows)
         if qmin is not None:
-            lines.append(f"lb {metric} {mk} {qmin} gemm   # {detail}")
+            lines.append(f"{kind} {metric} {mk} {qmin} gemm   # {detail}")
         else:
-            lines.append(f"# lb {metric} {mk}: fft at every measured size ({detail})")
+            lines.append(f"# {kind} {metric} {mk}: fft at every measured size ({detail})")
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
 

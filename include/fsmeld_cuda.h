@@ -148,7 +148,8 @@ int fsmeld_set_lb_form(fsmeld_ctx* ctx, int form);
 /* Tuning table for the automatic choices (no reference counterpart): one rule
  * per line, "kind metric m_k limit choice", first match wins, '#' comments.
  *   dp <metric> <m_k> <w_max>  lane|wave   exact DP kernel for w <= w_max
- *   lb <metric> <m_k> <q_min>  fft|gemm    LB_IP form for groups of >= q_min
+ *   lb <metric> <m_k> <q_min>  fft|gemm    LB_IP form for groups of >= q_min searches
+ *   lbk <metric> <m_k> <q_min> fft|gemm    the same for groups of top-k queries
  * Shapes no rule covers keep the built-in choice (the lane DP while its band
  * fits shared memory; the FFT LB_IP).  fsmeld_b200/tune.py measures the
  * rules on the GPU and writes fsmeld_b200/tune_table.txt, which the Python
