@@ -287,7 +287,7 @@ __device__ void trailing_phase(const double* __restrict__ src, int n, int B, int
 }  // namespace
 
 template <int T, int OPT, bool GW>
-__global__ void __launch_bounds__(T) k_envelope(const double* __restrict__ target,
+__global__ void __launch_bounds__(T, (T <= 512 ? 2 : 1)) k_envelope(const double* __restrict__ target,
                                                 const double* __restrict__ MU,
                                                 const double* __restrict__ SIG, Geom g, int w,
                                                 double* __restrict__ Un, double* __restrict__ Ln,
