@@ -217,7 +217,7 @@ struct fsmeld_ctx {
     // tuner's choice), 1 the per-query FFT form, 2 the tensor-core product
     int lb_form = 0;
     // tuning table (fsmeld_set_tuning): rules for the automatic choices
-    struct TuneRule { int kind, metric, m_k, lim, choice; };  // kind 0 dp, 1 lb (search), 2 lbk (top-k)
+    struct TuneRule { int kind, metric, m_k, lim, choice; };  // 0 dp, 1 lb (search), 2 lbk (top-k), 3 dpx (scan)
     std::vector<TuneRule> tune;
     // normalisation mode (the reference's set_normalization_mode, include/funcs.h:20-28):
     // false z-score (the reference CLI's only mode), true raw
@@ -607,13 +607,13 @@ static int run_glb(fsmeld_ctx* c, const Geom& g, const QueryDev& qd, const Stats
 }
 
 // The tuning table's choice for a shape: the first rule of `kind` for the
-// metric and macro-segment length whose limit is >= v (dp: v = w, choice
-// 1 lane / 2 wave; lb, lbk: v = the group's query count as a lower limit,
-// choice 1 fft / 2 gemm).  0 when no rule matches.
+// metric and macro-segment length whose limit matches v (dp, dpx: v = w <=
+// limit, choice 1 lane / 2 wave; lb, lbk: v = the group's query count >=
+// limit, choice 1 fft / 2 gemm).  0 when no rule matches.
 static int tuned(const fsmeld_ctx* c, int kind, int metric, int m_k, int v) {
     for (const auto& t : c->tune) {
         if (t.kind != kind || t.metric != metric || t.m_k != m_k) continue;
-        if (kind == 0 ? v <= t.lim : v >= t.lim) return t.choice;
+        if ((kind == 0 || kind == 3) ? v <= t.lim : v >= t.lim) return t.choice;
     }
     return 0;
 }
@@ -634,7 +634,7 @@ static int run_dp(fsmeld_ctx* c, const Geom& g, DpJob job, long long expected) {
     const bool gw_path = smem > (size_t)c->smem_optin - 4096;
     // wide bands (and FSMELD_DP_FORM=wave): one warp per candidate, band in registers
     int form = c->dp_form;
-    if (form == 0) form = tuned(c, 0, job.q.metric, g.m_k, w);
+    if (form == 0) form = tuned(c, job.list ? 0 : 3, job.q.metric, g.m_k, w);
     const void* wk = form == 1 ? nullptr : dpw_kernel(job.q.metric, w);
     const size_t wsm = dpw_smem_bytes(job.q.m, kDpwThreads / 32);
     if (wk && wsm + 1024 <= (size_t)c->smem_optin && (form == 2 || gw_path)) {
@@ -1627,7 +1627,8 @@ int fsmeld_set_tuning(fsmeld_ctx* c, const char* table) {
             return fail(FSMELD_E_ARG, "tuning table: a line is not 'kind metric m_k limit choice'");
         }
         fsmeld_ctx::TuneRule t{};
-        t.kind = !strcmp(kind, "dp") ? 0 : !strcmp(kind, "lb") ? 1 : !strcmp(kind, "lbk") ? 2 : -1;
+        t.kind = !strcmp(kind, "dp") ? 0 : !strcmp(kind, "lb") ? 1 : !strcmp(kind, "lbk") ? 2
+               : !strcmp(kind, "dpx") ? 3 : -1;
         t.metric = !strcmp(metric, "dtw") ? DTW : !strcmp(metric, "erp") ? ERP : !strcmp(metric, "edr") ? EDR
                  : !strcmp(metric, "lcss") ? LCSS : !strcmp(metric, "msm") ? MSM : -1;
         t.m_k = mk;

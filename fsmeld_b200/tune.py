@@ -2,11 +2,13 @@
 
 Two choices depend on the shape and are settled by measurement:
 
-* the exact DP kernel (`dp` rules): the lane-per-candidate DP (band and
-  candidate ring per lane in shared memory) or the anti-diagonal wavefront
-  (one warp per candidate, band in registers), per metric, macro-segment
-  length m_k and radius w.  Timed as the exact scan (every window through the
-  DP, early abandon at the query's rank-20 distance) on a seeded random walk.
+* the exact DP kernel: the lane-per-candidate DP (band and candidate ring
+  per lane in shared memory) or the anti-diagonal wavefront (one warp per
+  candidate, band in registers), per metric, macro-segment length m_k and
+  radius w; `dp` rules for the DP over the GLB survivors of a search or
+  top-k query (timed as a search at the rank-50 distance on a structured
+  walk), `dpx` rules for the exact scan of every window (timed at the
+  rank-20 distance on a random walk).
 * the LB_IP form of batched searches (`lb` rules) and top-k queries (`lbk`):
   per-query thresholds and FP64 FFTs, or one tensor-core product for the
   group, per metric, m_k and group size.  Timed as one batched `search` of
@@ -28,7 +30,7 @@ import time
 import numpy as np
 
 from fsmeld_b200 import api
-from fsmeld_b200.synth import query_from, random_walk
+from fsmeld_b200.synth import query_from, random_walk, walk_with_structure
 
 METRIC_ARGS = {"dtw": 0.0, "erp": 0.0, "edr": 0.25, "lcss": 0.25, "msm": 0.5}
 DP_SHAPES = {64: (2, 3, 6, 13, 31), 128: (3, 6, 13, 26, 51), 256: (6, 13, 26, 51, 94),
@@ -60,26 +62,41 @@ def timed(eng, fn, reps=2):
 
 
 def tune_dp(metrics, shapes, log):
+    """dp: the DP over a candidate list (search and top-k), timed as a search
+    at the query's rank-50 distance on a structured walk of 2^20 points (the
+    search's other stages are the same for both forms); dpx: the exact scan
+    (every window), timed at the rank-20 distance on 2^16-2^17 points."""
     rules = []
     for m, ws in shapes.items():
         n = (1 << 17) if m <= 256 else (1 << 16)
         t = random_walk(n, 9000 + m)
         q, _ = query_from(t, m, np.random.default_rng(9001 + m))
+        ts = walk_with_structure(1 << 20, m, seed=9002 + m, motifs=40, nan_fraction=1e-3, flat_runs=8)
+        qs, _ = query_from(ts, m, np.random.default_rng(9003 + m))
         for metric in metrics:
             arg = METRIC_ARGS[metric]
             for w in ws:
                 if w >= m or not lane_fits(w):
                     continue
-                times = {}
-                for form in ("lane", "wave"):
-                    table = f"dp {metric} {macro_length(m)} 1000 {form}\n"
-                    with api.Engine(t, tuning=table) as e:
-                        _, d, _ = e.cutoff(q, m, 20, metric, w, arg)
-                        cut = float(d[-1])
-                        times[form] = timed(e, lambda: e.exact(q, m, cut, metric, w, arg))
-                choice = min(times, key=times.get)
-                log(f"dp {metric} m={m} w={w}: lane {times['lane']:.2f} ms, wave {times['wave']:.2f} ms -> {choice}")
-                rules.append((metric, macro_length(m), w, choice, times))
+                mk = macro_length(m)
+                for kind in ("dp", "dpx"):
+                    times = {}
+                    for form in ("lane", "wave"):
+                        table = f"{kind} {metric} {mk} 1000 {form}\n"
+                        if kind == "dp":
+                            with api.Engine(ts, tuning=table) as e:
+                                _, d, _ = e.cutoff(qs, m, 50, metric, w, arg)
+                                cut = float(d[-1])
+                                times[form] = timed(e, lambda: e.search(qs, m, cut, metric, w, arg))
+                        else:
+                            with api.Engine(t, tuning=table) as e:
+                                _, d, _ = e.cutoff(q, m, 20, metric, w, arg)
+                                cut = float(d[-1])
+                                times[form] = timed(e, lambda: e.exact(q, m, cut, metric, w, arg))
+                    choice = min(times, key=times.get)
+                    log(f"{kind} {metric} m={m} w={w}: lane {times['lane']:.2f} ms, wave {times['wave']:.2f} ms "
+                        f"-> {choice}")
+                    rules.append((kind, metric, mk, w, choice, times))
     return rules
 
 
@@ -114,8 +131,8 @@ def tune_lb(metrics, shapes, log, n=1 << 22):
 def write_table(path, dp_rules, lb_rules):
     lines = ["# Tuning table: measured by `python -m fsmeld_b200.tune` on one B200.",
              "# kind metric m_k limit choice  (dp: w <= limit; lb: group size >= limit); first match wins"]
-    for metric, mk, w, choice, times in dp_rules:
-        lines.append(f"dp {metric} {mk} {w} {choice}   # lane {times['lane']:.2f} ms, wave {times['wave']:.2f} ms")
+    for kind, metric, mk, w, choice, times in dp_rules:
+        lines.append(f"{kind} {metric} {mk} {w} {choice}   # lane {times['lane']:.2f} ms, wave {times['wave']:.2f} ms")
     # lb: for each (metric, m_k) the smallest group size from which the product wins at every measured size
     by_shape = {}
     for kind, metric, mk, nq, choice, times in lb_rules:

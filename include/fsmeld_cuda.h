@@ -147,7 +147,9 @@ int fsmeld_set_lb_form(fsmeld_ctx* ctx, int form);
 
 /* Tuning table for the automatic choices (no reference counterpart): one rule
  * per line, "kind metric m_k limit choice", first match wins, '#' comments.
- *   dp <metric> <m_k> <w_max>  lane|wave   exact DP kernel for w <= w_max
+ *   dp <metric> <m_k> <w_max>  lane|wave   exact DP kernel over a candidate list
+ *                                          (search, top-k) for w <= w_max
+ *   dpx <metric> <m_k> <w_max> lane|wave   the same for the exact scan
  *   lb <metric> <m_k> <q_min>  fft|gemm    LB_IP form for groups of >= q_min searches
  *   lbk <metric> <m_k> <q_min> fft|gemm    the same for groups of top-k queries
  * Shapes no rule covers keep the built-in choice (the lane DP while its band
