@@ -169,53 +169,6 @@ __device__ __forceinline__ double dp_row(double* __restrict__ A, const double* _
     return ext;
 }
 
-// Two consecutive rows (i, i+1) in fast mode, interleaved with a lag of two
-// cells: at step t row i computes cell t and row i+1 cell t-2.  Cell d of
-// row i+1 reads row i's cells d (diagonal) and d+1 (above), both written one
-// and two steps earlier, and row i+1 overwrites row i's cell d in place only
-// after reading it, while row i still reads row i-1's cells at t+1 -- so the
-// band row holds each row's values exactly when the sequential order would,
-// every cell gets the same operands, and the two rows' dependency chains run
-// side by side.  s0: ring index of row i's cell 0 (row i+1's is s0 + 1).
-// extA / extB: the rows' minima (maxima for LCSS).
-template <int METRIC>
-__device__ __forceinline__ void dp_row2(double* __restrict__ A, const double* __restrict__ R, int RM, int W2,
-                                        int s0, const RowCtx& ra, const RowCtx& rb, double arg, double& extA,
-                                        double& extB) {
-    constexpr double SENT = (METRIC == LCSS) ? 0.0 : kDpMax;
-    double leftA = SENT, leftB = SENT, eA = SENT, eB = SENT;
-    double pdA = A[0];
-    double yprevA = (METRIC == MSM) ? R[((s0 - 1) & RM) * 32] : 0.0;
-    double yprevB = (METRIC == MSM) ? R[(s0 & RM) * 32] : 0.0;
-    double pdB = 0.0;  // row i's cell d (the diagonal of row i+1's cell d), read a step ahead
-    for (int t = 0; t < W2 + 2; ++t) {
-        if (t < W2) {
-            const double pn = A[(t + 1) * 32];
-            const double y = R[((s0 + t) & RM) * 32];
-            const double v = dp_cell<METRIC, false>(pn, pdA, leftA, y, yprevA, ra, arg, t, 0, 0, -1);
-            A[t * 32] = v;
-            leftA = v;
-            pdA = pn;
-            yprevA = y;
-            eA = (METRIC == LCSS) ? smax(eA, v) : smin(eA, v);
-        }
-        if (t >= 2) {
-            const int d = t - 2;
-            if (d == 0) pdB = A[0];
-            const double pn = A[(d + 1) * 32];
-            const double y = R[((s0 + 1 + d) & RM) * 32];
-            const double v = dp_cell<METRIC, false>(pn, pdB, leftB, y, yprevB, rb, arg, d, 0, 0, -1);
-            A[d * 32] = v;
-            leftB = v;
-            pdB = pn;
-            yprevB = y;
-            eB = (METRIC == LCSS) ? smax(eB, v) : smin(eB, v);
-        }
-    }
-    extA = eA;
-    extB = eB;
-}
-
 }  // namespace
 
 template <int METRIC, bool GW>
@@ -281,28 +234,17 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
     // inputs of the lane's next row, loaded one row ahead so that their
     // latency overlaps the current row: query points, the next raw candidate
     // point (held for index nty) and the cascade term's forward-window reads
-    // (the second set, suffix 2, holds the row after it for the two-row step)
     double nx = 0.0, nxp = 0.0, nt = 0.0, na0 = 0.0, na1 = 0.0, nb0 = 0.0, nb1 = 0.0;
-    double nx2 = 0.0, nt2 = 0.0, na20 = 0.0, na21 = 0.0, nb20 = 0.0, nb21 = 0.0;
-    int nty = -1, nty2 = -1;
+    int nty = -1;
     auto prefetch = [&](int r) {
         const int k = ONE_BASED ? r - 1 : r;
         nx = X[k];
         if (METRIC == MSM) nxp = (r > 0) ? X[r - 1] : -kPad;
         if (ny < m) { nt = tp[ny]; nty = ny; }
-        if (ny + 1 < m) { nt2 = tp[ny + 1]; nty2 = ny + 1; }
         if (has_s && (METRIC == LCSS || (k >= 1 && k <= m - 2))) {
             const int p0 = qt_p0(k, w), p1 = qt_p1(k, m, w);
             na0 = lr[p0]; na1 = lr[p1];
             nb0 = ur[p0]; nb1 = ur[p1];
-        }
-        if (k + 1 < m) {
-            nx2 = X[k + 1];
-            if (has_s && (METRIC == LCSS || (k + 1 >= 1 && k + 1 <= m - 2))) {
-                const int p0 = qt_p0(k + 1, w), p1 = qt_p1(k + 1, m, w);
-                na20 = lr[p0]; na21 = lr[p1];
-                nb20 = ur[p0]; nb21 = ur[p1];
-            }
         }
     };
 
@@ -311,7 +253,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
         for (; ny <= upto; ++ny) {
             double y = kPad;
             if (ny < m) {
-                y = zdiv(dsub(ny == nty ? nt : (ny == nty2 ? nt2 : tp[ny]), mu), sg, inv, rok);
+                y = zdiv(dsub(ny == nty ? nt : tp[ny], mu), sg, inv, rok);
                 over = over || !(fabs(y) <= ylim);
             }
             R[(ny & RM) * 32] = y;
@@ -489,7 +431,6 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
                     row = 1;
                 }
                 nty = -1;
-                nty2 = -1;
                 prefetch(row);
             }
         }
@@ -501,14 +442,10 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
 
         const int i = row;
         const int s0 = ONE_BASED ? i - w - 1 : i - w;  // ring index read by cell d = 0
-        // fast mode with two rows left: rows i and i+1 in one interleaved step
-        // (MSM also reads y_{s0-1}: the ring must hold 2w+3 points then)
-        const bool pair = !exact && i + 1 <= last && (METRIC != MSM || RING >= 2 * w + 3);
-        fill_ring(s0 + 2 * w + (pair ? 1 : 0));         // one new point per row in steady state
+        fill_ring(s0 + 2 * w);                          // one new point per row in steady state
         if (over && !exact) {                           // out of the fast-mode range: restart exact
             exact = true;
             nty = -1;
-            nty2 = -1;
             start();
             prefetch(row);
             continue;
@@ -532,53 +469,22 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
         // cascading-bound term of this row's query point (inputs loaded a row ahead)
         const bool use_term = has_s && (METRIC == LCSS || (k >= 1 && k <= m - 2));
         const double ta = fmin(na0, na1), tb = fmax(nb0, nb1);
-        // the second row of a pair: query point and cascade term of row i+1
-        RowCtx rb;
-        bool use_term2 = false;
-        double ta2 = 0.0, tb2 = 0.0;
-        if (pair) {
-            rb.xi = nx2;
-            rb.i = i + 1;
-            rb.c0 = 0.0;
-            rb.xp = rb.xi;
-            if (METRIC == ERP) rb.c0 = dsq(rb.xi, arg);
-            if (METRIC == MSM) {
-                rb.xp = rc.xi;
-                rb.c0 = fabs(dsub(rb.xi, rb.xp));
-            }
-            rb.ge = rb.xp <= rb.xi;
-            rb.le = rb.xi <= rb.xp;
-            use_term2 = has_s && (METRIC == LCSS || (k + 1 >= 1 && k + 1 <= m - 2));
-            ta2 = fmin(na20, na21);
-            tb2 = fmax(nb20, nb21);
-        }
-        const int nxt = i + (pair ? 2 : 1);
-        if (nxt <= last) prefetch(nxt);  // the next step's loads overlap this step's cells
+        if (i < last) prefetch(i + 1);  // next row's loads overlap this row's cells
         const double term = use_term ? qt_term_bound(METRIC, rc.xi, ta, tb, mu, inv, arg) : 0.0;
         double ext;
-        if (pair) {
-            double extA;
-            dp_row2<METRIC>(A, R, RM, W2, s0, rc, rb, arg, extA, ext);
-            if (use_term) Pre = dadd(Pre, term);
-            if (use_term2) Pre = dadd(Pre, qt_term_bound(METRIC, rb.xi, ta2, tb2, mu, inv, arg));
-            cells += 2ull * (unsigned long long)W2;
-            row = i + 1;  // the checks below see the pair's second row
+        if (!exact) {
+            ext = dp_row<METRIC, false>(A, R, RM, W2, s0, rc, arg, 0, 0, -1);
         } else {
-            if (!exact) {
-                ext = dp_row<METRIC, false>(A, R, RM, W2, s0, rc, arg, 0, 0, -1);
-            } else {
-                const int dlo = max(0, w - i), dhi = min(2 * w, last - i + w);
-                const int d0 = (METRIC == ERP || METRIC == EDR || METRIC == MSM) ? w - i : -1;
-                ext = dp_row<METRIC, true>(A, R, RM, W2, s0, rc, arg, dlo, dhi, d0);
-            }
-            if (use_term) Pre = dadd(Pre, term);
-            cells += (unsigned long long)W2;
+            const int dlo = max(0, w - i), dhi = min(2 * w, last - i + w);
+            const int d0 = (METRIC == ERP || METRIC == EDR || METRIC == MSM) ? w - i : -1;
+            ext = dp_row<METRIC, true>(A, R, RM, W2, s0, rc, arg, dlo, dhi, d0);
         }
-        const int ie = row;  // the last row done
+        if (use_term) Pre = dadd(Pre, term);
+        cells += (unsigned long long)W2;
 
         bool done = false, keep = false;
         double dist = 0.0;
-        if (ie == last) {
+        if (i == last) {
             const double fin = A[w * 32];
             if (METRIC == DTW || METRIC == ERP) dist = isfinite(fin) ? dsqrt(dmax0(fin)) : kDpMax;
             else if (METRIC == LCSS) dist = dsub(1.0, ddiv(fin, (double)m));
@@ -588,7 +494,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(Geom g, DpJob job) {
         } else if (METRIC == LCSS) {
             // remaining rows can add at most one match each, and only where the
             // query point meets the candidate envelope
-            double rest = (double)(m - 1 - ie);
+            double rest = (double)(m - 1 - i);
             if (has_s) rest = fmin(rest, fmax(0.0, dsub(Ssum, Pre)));
             if (dadd(ext, rest) < lcss_lim) done = true;
         } else {

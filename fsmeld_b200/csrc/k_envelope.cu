@@ -149,145 +149,10 @@ __device__ void minmax_phase(const double* __restrict__ src, int n, int par, int
     __syncthreads();
 }
 
-// Trailing windows [o-B+1, o] (min_max_window, B = m) by van Herk /
-// Gil-Werman with blocks of B: per block the prefix extrema P and suffix
-// extrema S, each block scanned by one warp (lanes own consecutive chunks,
-// a shuffle scan carries the chunk extrema), so the whole phase needs one
-// block barrier.  A window starting on a block boundary is P at its end, a
-// window inside one block (the segment's right edge) is S at its start, any
-// other is min(S[start], P[end]); windows holding a NaN are evaluated
-// directly as in minmax_phase.
-template <int T, int OPT>
-__device__ void trailing_phase(const double* __restrict__ src, int n, int B, int nout, const EnvWork& wk,
-                               EnvTemp<T>& tmp, double (&omn)[OPT], double (&omx)[OPT]) {
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    int local_nan = 0;
-    for (int i = t; i < n; i += T) {
-        const double v = src[i];
-        wk.raw[px(i)] = v;
-        local_nan |= isnan(v) ? 1 : 0;
-    }
-    const int any_nan = __syncthreads_or(local_nan);
-    if (any_nan) {
-        const int c = (n + T - 1) / T;
-        const int lo = t * c, hi = min(n, lo + c);
-        int cnt = 0;
-        for (int i = lo; i < hi; ++i) cnt += isnan(wk.raw[px(i)]) ? 1 : 0;
-        int off;
-        cub::BlockScan<int, T>(tmp.ic).ExclusiveSum(cnt, off);
-        for (int i = lo; i < hi; ++i) {
-            wk.ncnt[px(i)] = off;
-            off += isnan(wk.raw[px(i)]) ? 1 : 0;
-        }
-        if (hi == n && lo < hi) wk.ncnt[px(n)] = off;
-    }
-    const int nblk = (n + B - 1) / B;
-    for (int blk = warp; blk < nblk; blk += T / 32) {
-        const int b0 = blk * B, b1 = min(n, b0 + B);
-        const int c = (b1 - b0 + 31) / 32;
-        const int lo = min(b1, b0 + lane * c), hi = min(b1, lo + c);
-        // prefix within the chunk, then the carry of the chunks to the left
-        double rmn = 0.0, rmx = 0.0;
-        bool have = false;
-        for (int i = lo; i < hi; ++i) {
-            const double v = wk.raw[px(i)];
-            rmn = (!have || v < rmn) ? v : rmn;
-            rmx = (!have || v > rmx) ? v : rmx;
-            have = true;
-            wk.Pmn[px(i)] = rmn;
-            wk.Pmx[px(i)] = rmx;
-        }
-        double cmn = rmn, cmx = rmx;
-        bool chave = have;
-        for (int o = 1; o < 32; o <<= 1) {  // inclusive scan of the chunk extrema
-            const double pmn = __shfl_up_sync(0xffffffffu, cmn, o), pmx = __shfl_up_sync(0xffffffffu, cmx, o);
-            const bool ph = __shfl_up_sync(0xffffffffu, (int)chave, o) != 0;
-            if (lane >= o && ph) {
-                cmn = (!chave || pmn < cmn) ? pmn : cmn;
-                cmx = (!chave || pmx > cmx) ? pmx : cmx;
-                chave = true;
-            }
-        }
-        double emn = __shfl_up_sync(0xffffffffu, cmn, 1), emx = __shfl_up_sync(0xffffffffu, cmx, 1);
-        const bool eh = lane > 0 && __shfl_up_sync(0xffffffffu, (int)chave, 1) != 0;
-        if (eh)
-            for (int i = lo; i < hi; ++i) {
-                const double a = wk.Pmn[px(i)], x = wk.Pmx[px(i)];
-                wk.Pmn[px(i)] = (emn < a) ? emn : a;
-                wk.Pmx[px(i)] = (emx > x) ? emx : x;
-            }
-        // suffix within the chunk, then the carry of the chunks to the right
-        have = false;
-        for (int i = hi - 1; i >= lo; --i) {
-            const double v = wk.raw[px(i)];
-            rmn = (!have || v < rmn) ? v : rmn;
-            rmx = (!have || v > rmx) ? v : rmx;
-            have = true;
-            wk.Smn[px(i)] = rmn;
-            wk.Smx[px(i)] = rmx;
-        }
-        cmn = rmn; cmx = rmx; chave = have;
-        for (int o = 1; o < 32; o <<= 1) {
-            const double pmn = __shfl_down_sync(0xffffffffu, cmn, o), pmx = __shfl_down_sync(0xffffffffu, cmx, o);
-            const bool ph = __shfl_down_sync(0xffffffffu, (int)chave, o) != 0;
-            if (lane + o < 32 && ph) {
-                cmn = (!chave || pmn < cmn) ? pmn : cmn;
-                cmx = (!chave || pmx > cmx) ? pmx : cmx;
-                chave = true;
-            }
-        }
-        emn = __shfl_down_sync(0xffffffffu, cmn, 1);
-        emx = __shfl_down_sync(0xffffffffu, cmx, 1);
-        const bool fh = lane < 31 && __shfl_down_sync(0xffffffffu, (int)chave, 1) != 0;
-        if (fh)
-            for (int i = lo; i < hi; ++i) {
-                const double a = wk.Smn[px(i)], x = wk.Smx[px(i)];
-                wk.Smn[px(i)] = (emn < a) ? emn : a;
-                wk.Smx[px(i)] = (emx > x) ? emx : x;
-            }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < OPT; ++k) {
-        const int o = t + k * T;
-        double vmn = 0.0, vmx = 0.0;
-        if (o < nout) {
-            const int ws = max(0, o - B + 1), we = min(o, n - 1);
-            if (any_nan && (wk.ncnt[px(we + 1)] - wk.ncnt[px(ws)] > 0)) {
-                const double a = wk.raw[px(ws)];
-                vmn = a;
-                vmx = a;
-                if (!isnan(a)) {
-                    for (int i = ws + 1; i <= we; ++i) {
-                        const double v = wk.raw[px(i)];
-                        if (isnan(v)) break;
-                        vmn = (v <= vmn) ? v : vmn;
-                        vmx = (v >= vmx) ? v : vmx;
-                    }
-                }
-            } else if (ws % B == 0) {
-                vmn = wk.Pmn[px(we)];
-                vmx = wk.Pmx[px(we)];
-            } else if (ws / B == we / B) {
-                vmn = wk.Smn[px(ws)];
-                vmx = wk.Smx[px(ws)];
-            } else {
-                const double pm = wk.Pmn[px(we)], sm = wk.Smn[px(ws)];
-                const double pxv = wk.Pmx[px(we)], sx = wk.Smx[px(ws)];
-                vmn = (pm < sm) ? pm : sm;
-                vmx = (pxv > sx) ? pxv : sx;
-            }
-        }
-        omn[k] = vmn;
-        omx[k] = vmx;
-    }
-    __syncthreads();
-}
-
 }  // namespace
 
 template <int T, int OPT, bool GW>
-__global__ void __launch_bounds__(T, (T <= 512 ? 2 : 1)) k_envelope(const double* __restrict__ target,
+__global__ void __launch_bounds__(T) k_envelope(const double* __restrict__ target,
                                                 const double* __restrict__ MU,
                                                 const double* __restrict__ SIG, Geom g, int w,
                                                 double* __restrict__ Un, double* __restrict__ Ln,
@@ -306,8 +171,8 @@ __global__ void __launch_bounds__(T, (T <= 512 ? 2 : 1)) k_envelope(const double
     wk.ncnt = (int*)(base + 5 * pk);
     for (long long s = blockIdx.x; s < g.S; s += gridDim.x) {
         double simn[OPT], simx[OPT], mumn[OPT], mumx[OPT], lmn[OPT], lmx[OPT];
-        trailing_phase<T, OPT>(SIG + s * kml, kml, m, mk, wk, tmp, simn, simx);
-        trailing_phase<T, OPT>(MU + s * kml, kml, m, mk, wk, tmp, mumn, mumx);
+        minmax_phase<T, OPT, false>(SIG + s * kml, kml, m, mk, wk, tmp, simn, simx);
+        minmax_phase<T, OPT, false>(MU + s * kml, kml, m, mk, wk, tmp, mumn, mumx);
         minmax_phase<T, OPT, true>(target + g.off(s), mk, w, mk, wk, tmp, lmn, lmx);
 #pragma unroll
         for (int k = 0; k < OPT; ++k) {
