@@ -24,6 +24,8 @@
 #include <string>
 #include <vector>
 
+#include <unistd.h>
+
 #include "../../include/fsmeld_cuda.h"
 
 namespace {
@@ -154,9 +156,24 @@ int setup(const char* tp, const char* qp, int m, Setup* s) {
     }
     s->n = fsmeld_target_length(s->ctx);
     if (raw_mode()) fsmeld_set_normalization(s->ctx, FSMELD_NORM_RAW);
-    // FSMELD_TUNE_TABLE: a tuning table file (fsmeld_set_tuning) for the kernel choices
+    // FSMELD_TUNE_TABLE: a tuning table file (fsmeld_set_tuning) for the kernel
+    // choices; by default the package's measured table beside the bin/ folder
+    // of this executable, when present
+    std::string table;
     if (const char* tp_env = std::getenv("FSMELD_TUNE_TABLE")) {
-        if (FILE* tf = fopen(tp_env, "r")) {
+        table = tp_env;
+    } else {
+        char exe[4096];
+        const ssize_t len = readlink("/proc/self/exe", exe, sizeof(exe) - 1);
+        if (len > 0) {
+            exe[len] = 0;
+            std::string dir(exe);
+            dir = dir.substr(0, dir.rfind('/'));         // .../bin
+            table = dir.substr(0, dir.rfind('/')) + "/tune_table.txt";
+        }
+    }
+    if (!table.empty()) {
+        if (FILE* tf = fopen(table.c_str(), "r")) {
             std::string text;
             char buf[4096];
             size_t got;

@@ -15,16 +15,21 @@ Two choices depend on the shape and are settled by measurement:
   the group at each query's rank-10 distance, and one batched `cutoff` k=10,
   on a 2^22-point random walk.
 
-Shapes where the lane DP's band does not fit shared memory need no
-measurement (the wavefront is the only shared-memory form there).  The table
-(fsmeld_b200/tune_table.txt) is loaded by api.Engine into every context.
+A rule departs from the built-in choice (lane DP, FFT LB_IP) only where the
+other form measured at least MARGIN (5%) faster, so timing noise between two
+nearly equal forms does not flip a shape back and forth.  Shapes where the
+lane DP's band does not fit shared memory need no measurement (the wavefront
+is the only shared-memory form there).  The table (fsmeld_b200/tune_table.txt)
+is loaded by api.Engine into every context.
 
     python -m fsmeld_b200.tune [--quick] [--out PATH]
+    python -m fsmeld_b200.tune --from-log LOG [--out PATH]   # table from a measurement log
 """
 from __future__ import annotations
 
 import argparse
 import os
+import re
 import time
 
 import numpy as np
@@ -36,6 +41,15 @@ METRIC_ARGS = {"dtw": 0.0, "erp": 0.0, "edr": 0.25, "lcss": 0.25, "msm": 0.5}
 DP_SHAPES = {64: (2, 3, 6, 13, 31), 128: (3, 6, 13, 26, 51), 256: (6, 13, 26, 51, 94),
              512: (13, 26, 51, 94), 1024: (26, 51, 94), 2048: (51, 94)}
 LB_SHAPES = {128: (8, 32), 256: (8, 32), 512: (8, 32)}
+MARGIN = 0.05
+DEFAULT = {"dp": "lane", "dpx": "lane", "lb": "fft", "lbk": "fft"}
+
+
+def choose(kind, times):
+    """The built-in form unless the other one measured MARGIN faster."""
+    base = DEFAULT[kind]
+    other = min((f for f in times if f != base), key=times.get)
+    return other if times[other] < (1.0 - MARGIN) * times[base] else base
 
 
 def macro_length(m):
@@ -93,7 +107,7 @@ def tune_dp(metrics, shapes, log):
                                 _, d, _ = e.cutoff(q, m, 20, metric, w, arg)
                                 cut = float(d[-1])
                                 times[form] = timed(e, lambda: e.exact(q, m, cut, metric, w, arg))
-                    choice = min(times, key=times.get)
+                    choice = choose(kind, times)
                     log(f"{kind} {metric} m={m} w={w}: lane {times['lane']:.2f} ms, wave {times['wave']:.2f} ms "
                         f"-> {choice}")
                     rules.append((kind, metric, mk, w, choice, times))
@@ -121,7 +135,7 @@ def tune_lb(metrics, shapes, log, n=1 << 22):
                         for form in ("fft", "gemm"):
                             e.set_lb_form(form)
                             times[form] = timed(e, lambda: e.batch(mode, qs[:nq]))
-                        choice = min(times, key=times.get)
+                        choice = choose(kind, times)
                         log(f"{kind} {metric} m={m} q={nq}: fft {times['fft']:.2f} ms, gemm {times['gemm']:.2f} ms "
                             f"-> {choice}")
                         rules.append((kind, metric, macro_length(m), nq, choice, times))
@@ -130,7 +144,8 @@ def tune_lb(metrics, shapes, log, n=1 << 22):
 
 def write_table(path, dp_rules, lb_rules):
     lines = ["# Tuning table: measured by `python -m fsmeld_b200.tune` on one B200.",
-             "# kind metric m_k limit choice  (dp: w <= limit; lb: group size >= limit); first match wins"]
+             "# kind metric m_k limit choice  (dp: w <= limit; lb: group size >= limit); first match wins",
+             f"# a rule departs from the built-in form only where the other measured {MARGIN:.0%} faster"]
     for kind, metric, mk, w, choice, times in dp_rules:
         lines.append(f"{kind} {metric} {mk} {w} {choice}   # lane {times['lane']:.2f} ms, wave {times['wave']:.2f} ms")
     # lb: for each (metric, m_k) the smallest group size from which the product wins at every measured size
@@ -153,11 +168,36 @@ def write_table(path, dp_rules, lb_rules):
         f.write("\n".join(lines) + "\n")
 
 
+LOG_LINE = re.compile(r"^(dpx?|lbk?) (\w+) m=(\d+) (w|q)=(\d+): (\w+) ([\d.]+) ms, (\w+) ([\d.]+) ms")
+
+
+def rules_from_log(path):
+    """dp and lb rules from the lines a measurement run logged (the choices
+    are made again under the current margin)."""
+    dp, lb = [], []
+    with open(path) as f:
+        for ln in f:
+            mt = LOG_LINE.match(ln)
+            if not mt:
+                continue
+            kind, metric, m, _, lim, f1, t1, f2, t2 = mt.groups()
+            times = {f1: float(t1), f2: float(t2)}
+            rule = (kind, metric, macro_length(int(m)), int(lim), choose(kind, times), times)
+            (dp if kind.startswith("dp") else lb).append(rule)
+    return dp, lb
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=api.TUNE_TABLE)
     ap.add_argument("--quick", action="store_true", help="DTW and MSM only")
+    ap.add_argument("--from-log", help="write the table from the lines of an earlier run's log")
     args = ap.parse_args()
+    if args.from_log:
+        dp, lb = rules_from_log(args.from_log)
+        write_table(args.out, dp, lb)
+        print(f"wrote {args.out} from {args.from_log}: {len(dp)} dp rules, {len(lb)} lb measurements")
+        return
     metrics = ["dtw", "msm"] if args.quick else list(METRIC_ARGS)
     t0 = time.time()
     log = lambda s: print(s, flush=True)  # noqa: E731
