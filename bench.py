@@ -162,22 +162,28 @@ FP64_PEAK_TOPS = 148 * 64 * 1.965e9 / 1e12
 
 
 def roofline(stages, cells, peaks):
-    """The dominant kernel, the exact DP (k_dp), is FP64-bound: algorithmic work
-    = band cells it computed (device counter; early abandon skips the rest) x
+    """The dominant kernel, the exact DP, is FP64-bound: algorithmic work =
+    band cells it computed (device counter; early abandon skips the rest) x
     FP64 operations per cell of the reference's recurrence, over its average
-    launch time."""
-    ms, launches = stages["k_dp"]
+    launch time.  The lane DP (k_dp) and the wavefront (k_dpw, where the
+    tuning table selects it) share the counter, so their launches are taken
+    together."""
+    ms_lane, n_lane = stages.get("k_dp", (0.0, 0))
+    ms_wave, n_wave = stages.get("k_dpw", (0.0, 0))
+    ms, launches = ms_lane + ms_wave, n_lane + n_wave
+    if launches == 0 or ms <= 0.0:
+        return None
+    kernel = "k_dp" if n_wave == 0 else ("k_dpw" if n_lane == 0 else "k_dp+k_dpw")
     flops = sum(cells[mt] * FLOPS_PER_CELL[mt] for mt in cells)
-    launches = max(1, launches)
     avg_s = ms / launches / 1e3
     achieved = flops / launches / avg_s / 1e12
     traffic = None
     try:
         with open(PROFILE_SUMMARY) as f:
-            traffic = json.load(f).get("k_dp", {}).get("bytes_per_launch")
+            traffic = json.load(f).get(kernel, {}).get("bytes_per_launch")
     except Exception:
         pass
-    return {"bound": "fp64", "kernel": "k_dp", "achieved": round(achieved, 3), "peak": round(FP64_PEAK_TOPS, 2),
+    return {"bound": "fp64", "kernel": kernel, "achieved": round(achieved, 3), "peak": round(FP64_PEAK_TOPS, 2),
             "unit": "TFLOP/s", "frac": round(achieved / FP64_PEAK_TOPS, 4), "traffic": traffic,
             "algorithmic_flops_per_launch": flops / launches, "avg_launch_ms": round(avg_s * 1e3, 4),
             "dp_cells_per_launch": sum(cells.values()) / launches, "flops_per_cell": FLOPS_PER_CELL,
@@ -368,13 +374,13 @@ def impl_ours(args):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
-    target, queries = make_workload(rank, args.n_points)
+    target, queries = make_workload(rank, args.n_points or N_POINTS)
     geom = geometry(len(target), M)
     eng = api.Engine(target, device=local)
     conc = args.concurrency or DEFAULT_CONCURRENCY
     eng.set_concurrency(conc)
     metrics = [(mt, ag) for mt, ag in METRICS if args.case in (None, mt)]
-    if args.case or args.fixed_cutoffs or args.n_points != N_POINTS:
+    if args.case or args.fixed_cutoffs or (args.n_points or N_POINTS) != N_POINTS:
         cutoffs = dict(CUTOFFS)  # profiling cases: the workload's constants, no setup launches
         cutoffs_match = None
     else:
@@ -479,7 +485,7 @@ def impl_ours(args):
             "data": "synthetic (seeded random walks with motifs, NaN spans and flat runs; stands in for the "
                     "reference's recorded datasets)",
             "config": {"workload": WORKLOAD if not args.case else f"{args.case} query of: {WORKLOAD}",
-                       "n": args.n_points, "m": M, "w": W, "k": K_TOP,
+                       "n": args.n_points or N_POINTS, "m": M, "w": W, "k": K_TOP,
                        "queries_per_step": len(metrics), "parallelism": f"{world} GPU(s), one target partition each",
                        "l2": "inputs larger than L2 (134 MB target per GPU)",
                        "cutoffs": cutoffs, "cutoffs_source": "reference k=50 distances (tests/golden/config_pins.json)",
@@ -497,7 +503,7 @@ def impl_ours(args):
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
-        if world == 1 and not args.no_cpu_baseline and not args.case and args.n_points == N_POINTS:
+        if world == 1 and not args.no_cpu_baseline and not args.case and (args.n_points or N_POINTS) == N_POINTS:
             line["cpu_baseline"] = cpu_baseline_single(target, queries, cutoffs)
         print(json.dumps(line))
     eng.close()
@@ -524,7 +530,7 @@ def workload_c4(args):
     from fsmeld_b200 import api
     from fsmeld_b200.synth import query_from, walk_with_bursts
 
-    n = args.n_points if args.n_points != N_POINTS else (1 << 27)
+    n = args.n_points or (1 << 27)
     t = walk_with_bursts(n, C4_M, seed=4)
     rng = np.random.default_rng(404)
     qs = [query_from(t, C4_M, rng)[0] for _ in range(args.queries)]
@@ -615,7 +621,7 @@ def workload_c3(args):
     from fsmeld_b200 import api
     from fsmeld_b200.synth import random_walk
 
-    n = args.n_points if args.n_points != N_POINTS else (1 << 26)
+    n = args.n_points or (1 << 26)
     count = args.queries if args.queries != 32 else 512
     t = random_walk(n, 3)
     qs = c3_queries(t, count)
@@ -734,10 +740,15 @@ def workload_c5(args):
         left = [len(reqs)]
         lk = threading.Lock()
 
+        errors = []
+
         def finish(i, t0):
             def cb(f):
                 lat[i] = time.perf_counter() - t0
                 answers[i] = f.result()[0] if f.exception() is None else None
+                if f.exception() is not None and len(errors) < 5:
+                    r = reqs[i]
+                    errors.append(f"{r[0]} m={r[2]} w={r[4]} {r[3]}: {f.exception()}")
                 with lk:
                     left[0] -= 1
                     if left[0] == 0:
@@ -779,7 +790,7 @@ def workload_c5(args):
             "latency_ms": {"p50": round(float(np.percentile(lat_ms, 50)), 2),
                            "p99": round(float(np.percentile(lat_ms, 99)), 2),
                            "max": round(float(lat_ms.max()), 2)},
-            "failed": failed, "answers_checked_against_alone": checked,
+            "failed": failed, "failures": errors, "answers_checked_against_alone": checked,
             "cutoff_precompute_s": round(t_pre, 1)}
     print(json.dumps(line))
     return 0
@@ -796,7 +807,7 @@ def workload_stream(args):
     from fsmeld_b200 import api
     from fsmeld_b200.stream import StreamingTarget, chunk_plan
 
-    target, queries = make_workload(0, args.n_points)
+    target, queries = make_workload(0, args.n_points or N_POINTS)
     batch = [dict(query=queries[mt], m=M, metric=mt, w=W, arg=ag, cutoff=CUTOFFS[mt]) for mt, ag in METRICS]
     path = os.path.join(tempfile.mkdtemp(), "target.bin")
     target.astype("<f8").tofile(path)
@@ -835,7 +846,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--case", choices=[m for m, _ in METRICS], help="one metric's query only (profiling runs)")
-    ap.add_argument("--n-points", type=int, default=N_POINTS, help="target length (profiling runs)")
+    ap.add_argument("--n-points", type=int, default=None,
+                    help="target length (default: the workload's own: 2^24 search5/stream, 2^26 c3, 2^27 c4)")
     ap.add_argument("--workload", choices=["search5", "c3", "c4", "c5", "stream"], default="search5",
                     help="c3: 512 mixed queries, batched vs plain (queries/s); "
                          "c4: batched DTW top-k queries over a 2^27-point target (queries/s); "

@@ -80,6 +80,8 @@ def lib():
             "fsmeld_last_error": (C.c_char_p, [ctxp]),
             "fsmeld_strerror": (C.c_char_p, [C.c_int]),
             "fsmeld_set_workspace_limit": (C.c_int, [ctxp, C.c_int64]),
+            "fsmeld_workspace_bytes": (C.c_int64, [ctxp]),
+            "fsmeld_release_workspace": (C.c_int, [ctxp]),
             "fsmeld_set_concurrency": (C.c_int, [ctxp, C.c_int]),
             "fsmeld_set_normalization": (C.c_int, [ctxp, C.c_int]),
             "fsmeld_set_lb_form": (C.c_int, [ctxp, C.c_int]),
@@ -220,6 +222,14 @@ class Engine:
 
     def set_workspace_limit(self, nbytes):
         _check(lib().fsmeld_set_workspace_limit(self._ctx, int(nbytes)), self._ctx)
+
+    def workspace_bytes(self):
+        """Device workspace bytes this engine holds now (its batch workers included)."""
+        return int(lib().fsmeld_workspace_bytes(self._ctx))
+
+    def release_workspace(self):
+        """Free the engine's workspace; the target stays resident."""
+        _check(lib().fsmeld_release_workspace(self._ctx), self._ctx)
 
     def set_concurrency(self, queries):
         """Queries of one (m, w) group of a batch run concurrently on this many streams."""

@@ -198,6 +198,11 @@ struct fsmeld_ctx {
     int sm_count = 148;
     int smem_optin = 227 * 1024;
     long long ws_limit = 0;
+    // worker contexts point at the context that created them; workspace
+    // bytes are counted and capped over the whole family (the context and
+    // its workers) under the root's mutex
+    fsmeld_ctx* parent = nullptr;
+    std::mutex ws_mu;
     long long launches = 0;
     // queries of one batch group run concurrently on this many worker
     // contexts (own stream and buffers, shared target, statistics, envelopes)
@@ -244,13 +249,37 @@ static size_t ws_total(const fsmeld_ctx* c) {
     return t;
 }
 
+static fsmeld_ctx* ws_root(fsmeld_ctx* c) {
+    while (c->parent) c = c->parent;
+    return c;
+}
+
+// workspace bytes of a context and its workers (and theirs); the caller
+// holds the root's ws_mu
+static size_t ws_family_total(const fsmeld_ctx* c) {
+    size_t t = ws_total(c);
+    for (const fsmeld_ctx* w : c->workers) t += ws_family_total(w);
+    return t;
+}
+
+// frees every workspace buffer of c (after its stream's work is done)
+static void release_bufs(fsmeld_ctx* c) {
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    std::lock_guard<std::mutex> lk(ws_root(c)->ws_mu);
+    for (auto& kv : c->bufs)
+        if (kv.second.p) cudaFree(kv.second.p);
+    c->bufs.clear();
+}
+
 static int buf(fsmeld_ctx* c, const std::string& name, size_t bytes, void** out) {
     if (bytes == 0) bytes = 16;
+    fsmeld_ctx* root = ws_root(c);
+    std::lock_guard<std::mutex> lk(root->ws_mu);
     auto& b = c->bufs[name];
     if (b.bytes < bytes) {
         if (b.p) { cudaFree(b.p); b.p = nullptr; b.bytes = 0; }
         const size_t want = bytes + bytes / 8;
-        if (c->ws_limit > 0 && (long long)(ws_total(c) + want) > c->ws_limit)
+        if (root->ws_limit > 0 && (long long)(ws_family_total(root) + want) > root->ws_limit)
             return fail(FSMELD_E_NOMEM, "Device workspace budget exceeded.");
         cudaError_t e = cudaMalloc(&b.p, want);
         if (e != cudaSuccess) { b.p = nullptr; return cuda_fail(e, "cudaMalloc", __FILE__, __LINE__); }
@@ -1136,8 +1165,21 @@ static int run_search_gemm(fsmeld_ctx* c, const Geom& g0, Stats& st, const std::
         const void* kf = lbgemm_kernel(NQ);
         const size_t smem = lbgemm_smem_bytes(NQ, m);
         if ((r = allow_smem(c, kf, smem))) return r;
+        // resident CTAs per SM from the kernel's own resources: shared memory
+        // (dynamic + static + the 1 KB the SM reserves per block), registers,
+        // threads, and TMEM (512 columns per SM, 2 NQ (>= 32) per CTA)
         int per_sm = 0;
-        FSM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf, kLbGemmThreads, smem));
+        {
+            cudaFuncAttributes fa;
+            FSM_CUDA_TRY(cudaFuncGetAttributes(&fa, kf));
+            int smem_sm = 0, regs_sm = 0, thr_sm = 0;
+            FSM_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device));
+            FSM_CUDA_TRY(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, c->device));
+            FSM_CUDA_TRY(cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, c->device));
+            const size_t per_block = smem + fa.sharedSizeBytes + 1024;
+            per_sm = (int)std::min<size_t>((size_t)smem_sm / per_block, (size_t)thr_sm / kLbGemmThreads);
+            if (fa.numRegs > 0) per_sm = std::min(per_sm, regs_sm / (fa.numRegs * kLbGemmThreads));
+        }
         const int cols = std::max(32, 2 * NQ);
         per_sm = std::max(1, std::min(per_sm, 512 / cols));  // TMEM: 512 columns per SM
         const long long items = g0.S * ((g0.kml + 127) / 128);
@@ -1229,6 +1271,7 @@ static int run_search_gemm(fsmeld_ctx* c, const Geom& g0, Stats& st, const std::
 static int get_worker(fsmeld_ctx* c, int i, fsmeld_ctx** out) {
     while ((int)c->workers.size() <= i) {
         fsmeld_ctx* w = new fsmeld_ctx();
+        w->parent = c;
         w->device = c->device;
         w->sm_count = c->sm_count;
         w->smem_optin = c->smem_optin;
@@ -1241,6 +1284,7 @@ static int get_worker(fsmeld_ctx* c, int i, fsmeld_ctx** out) {
             delete w;
             return fail(FSMELD_E_CUDA, "stream/event creation failed");
         }
+        std::lock_guard<std::mutex> lk(ws_root(c)->ws_mu);
         c->workers.push_back(w);
     }
     fsmeld_ctx* w = c->workers[i];
@@ -1270,6 +1314,7 @@ static int group_gemm(fsmeld_ctx* c, const Geom& g, Stats& st, std::vector<Query
         std::vector<size_t> idx;
         for (size_t k = gi; k < gj; ++k) {
             const QueryRun& qr = runs[order[k]];
+            if ((*done)[k]) continue;  // already answered
             if (qr.mode == mode && qr.hq->metric == metric) { qs.push_back(&qr); idx.push_back(k); }
         }
         if (qs.size() < 2) continue;
@@ -1317,54 +1362,82 @@ static int run_tasks_parallel(fsmeld_ctx* c, std::vector<QueryRun>& runs, const 
     std::atomic<size_t> next{0};
     std::atomic<bool> cuda_dead{false};
     std::vector<std::string> errs(conc);
+    // task ti on worker wk; retry: only the task's queries whose status is
+    // FSMELD_E_NOMEM (the statistics and envelopes are computed again)
+    auto run_task = [&](fsmeld_ctx* wk, size_t ti, bool retry, std::string& err) {
+        const size_t lo = tasks[ti].first, hi = tasks[ti].second;
+        auto wanted = [&](size_t k) { return !retry || (*status)[order[k]] == FSMELD_E_NOMEM; };
+        auto mark = [&](size_t a, size_t b, int code) {
+            for (size_t k = a; k < b; ++k)
+                if (wanted(k)) (*status)[order[k]] = code;
+            if (err.empty()) err = g_last_error;
+            if (code == FSMELD_E_CUDA) cuda_dead = true;
+        };
+        Geom g{};
+        Stats st;
+        int q = make_geom(c->n, runs[order[lo]].hq->m, -1, -1, &g);
+        g.raw = c->raw ? 1 : 0;
+        if (!q) q = run_stats(wk, g, &st, "");
+        if (q) { mark(lo, hi, q); return; }
+        size_t gi = lo;
+        while (gi < hi) {
+            const int w = runs[order[gi]].hq->w;
+            size_t gj = gi + 1;
+            while (gj < hi && runs[order[gj]].hq->w == w) ++gj;
+            bool need_env = false, any = false;
+            for (size_t k = gi; k < gj; ++k) {
+                need_env = need_env || runs[order[k]].mode != 2;
+                any = any || wanted(k);
+            }
+            if (!any) { gi = gj; continue; }
+            if (need_env && (q = run_env(wk, g, w, &st, ""))) { mark(gi, gj, q); gi = gj; continue; }
+            std::vector<char> done(hi, 0);
+            for (size_t k = gi; k < gj; ++k) done[k] = !wanted(k);
+            if ((q = group_gemm(wk, g, st, runs, order, gi, gj, status, &done, false)) == FSMELD_E_CUDA) {
+                mark(gi, gj, q);
+                break;
+            }
+            for (size_t k = gi; k < gj; ++k) {
+                if (done[k]) continue;
+                q = run_query(wk, runs[order[k]], g, st, need_env);
+                (*status)[order[k]] = q;
+                if (q && err.empty()) err = g_last_error;
+                if (q == FSMELD_E_CUDA) { cuda_dead = true; break; }
+            }
+            if (cuda_dead.load()) break;
+            gi = gj;
+        }
+    };
     std::vector<std::thread> th;
     for (int t = 0; t < conc; ++t) {
         th.emplace_back([&, t] {
             cudaSetDevice(c->device);
-            fsmeld_ctx* wk = ws[t];
             for (;;) {
                 const size_t ti = next.fetch_add(1);
                 if (ti >= tasks.size() || cuda_dead.load()) break;
-                const size_t lo = tasks[ti].first, hi = tasks[ti].second;
-                auto mark = [&](size_t a, size_t b, int code) {
-                    for (size_t k = a; k < b; ++k) (*status)[order[k]] = code;
-                    if (errs[t].empty()) errs[t] = g_last_error;
-                    if (code == FSMELD_E_CUDA) cuda_dead = true;
-                };
-                Geom g{};
-                Stats st;
-                int q = make_geom(c->n, runs[order[lo]].hq->m, -1, -1, &g);
-                g.raw = c->raw ? 1 : 0;
-                if (!q) q = run_stats(wk, g, &st, "");
-                if (q) { mark(lo, hi, q); continue; }
-                size_t gi = lo;
-                while (gi < hi) {
-                    const int w = runs[order[gi]].hq->w;
-                    size_t gj = gi + 1;
-                    while (gj < hi && runs[order[gj]].hq->w == w) ++gj;
-                    bool need_env = false;
-                    for (size_t k = gi; k < gj; ++k) need_env = need_env || runs[order[k]].mode != 2;
-                    if (need_env && (q = run_env(wk, g, w, &st, ""))) { mark(gi, gj, q); gi = gj; continue; }
-                    std::vector<char> done(hi, 0);
-                    if ((q = group_gemm(wk, g, st, runs, order, gi, gj, status, &done, false)) == FSMELD_E_CUDA) {
-                        mark(gi, gj, q);
-                        break;
-                    }
-                    for (size_t k = gi; k < gj; ++k) {
-                        if (done[k]) continue;
-                        q = run_query(wk, runs[order[k]], g, st, need_env);
-                        (*status)[order[k]] = q;
-                        if (q) mark(k, k + 1, q);
-                        if (q == FSMELD_E_CUDA) break;
-                    }
-                    if (cuda_dead.load()) break;
-                    gi = gj;
-                }
+                run_task(ws[t], ti, false, errs[t]);
             }
         });
     }
     for (auto& x : th) x.join();
     for (int t = 0; t < conc; ++t) absorb_worker(c, ws[t]);
+    // Queries refused for workspace while other tasks held theirs run again
+    // one task at a time on the first worker, after every worker's buffers
+    // are released; a query that still does not fit keeps FSMELD_E_NOMEM.
+    bool nomem = false;
+    for (size_t k = 0; k < order.size(); ++k) nomem = nomem || (*status)[order[k]] == FSMELD_E_NOMEM;
+    if (nomem && !cuda_dead.load()) {
+        for (int t = 0; t < conc; ++t) release_bufs(ws[t]);
+        for (size_t ti = 0; ti < tasks.size() && !cuda_dead.load(); ++ti) {
+            bool any = false;
+            for (size_t k = tasks[ti].first; k < tasks[ti].second; ++k)
+                any = any || (*status)[order[k]] == FSMELD_E_NOMEM;
+            if (!any) continue;
+            errs[0].clear();
+            run_task(ws[0], ti, true, errs[0]);
+        }
+        absorb_worker(c, ws[0]);
+    }
     int first_err = FSMELD_OK;
     for (size_t k = 0; k < order.size() && !first_err; ++k) first_err = (*status)[order[k]];
     if (first_err)
@@ -1474,6 +1547,24 @@ int run_batch(fsmeld_ctx* c, std::vector<QueryRun>& runs, std::vector<int>* stat
             // a query that failed part-way may have left kernels queued: the next
             // group rewrites the shared statistics only after they are done
             for (int t = 0; t < conc; ++t) absorb_worker(c, ws[t]);
+            // queries refused for workspace while the others held theirs run
+            // again one after another on this context, the workers' buffers
+            // released first; one that still does not fit keeps FSMELD_E_NOMEM
+            bool nomem = false, dead = false;
+            for (size_t k : rest) {
+                nomem = nomem || (*status)[k] == FSMELD_E_NOMEM;
+                dead = dead || (*status)[k] == FSMELD_E_CUDA;
+            }
+            if (nomem && !dead) {
+                for (int t = 0; t < conc; ++t) release_bufs(ws[t]);
+                for (size_t k : rest) {
+                    if ((*status)[k] != FSMELD_E_NOMEM) continue;
+                    const int q = run_query(c, runs[k], g, st, have_env);
+                    (*status)[k] = q;
+                    if (q) errs[0] = g_last_error;
+                    if (q == FSMELD_E_CUDA) break;
+                }
+            }
             for (size_t k = oi; k < oj; ++k) {
                 const int q = (*status)[order[k]];
                 if (q && !first_err) {
@@ -1647,6 +1738,25 @@ int fsmeld_set_lb_form(fsmeld_ctx* c, int form) {
     if (!c || form < FSMELD_LB_AUTO || form > FSMELD_LB_GEMM)
         return fail(FSMELD_E_ARG, "LB_IP form must be FSMELD_LB_AUTO, FSMELD_LB_FFT or FSMELD_LB_GEMM");
     c->lb_form = form;
+    return FSMELD_OK;
+}
+
+int64_t fsmeld_workspace_bytes(fsmeld_ctx* c) {
+    if (!c) return 0;
+    fsmeld_ctx* root = ws_root(c);
+    std::lock_guard<std::mutex> lk(root->ws_mu);
+    return (int64_t)ws_family_total(c);
+}
+
+static void release_family(fsmeld_ctx* c) {
+    for (fsmeld_ctx* w : c->workers) release_family(w);
+    release_bufs(c);
+}
+
+int fsmeld_release_workspace(fsmeld_ctx* c) {
+    if (!c) return fail(FSMELD_E_ARG, "null context");
+    cudaSetDevice(c->device);
+    release_family(c);
     return FSMELD_OK;
 }
 

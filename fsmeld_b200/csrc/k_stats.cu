@@ -21,8 +21,9 @@
 // Work split: warp 0 of the block runs the 32 running-sum chains (the serial
 // part) and stages each emitted window's sums and non-finite flag in a
 // double-buffered tile; warps 1-3 turn the previous tile's sums into mean
-// and sigma (two divisions and a square root per window, independent of
-// each other) and write them out, so the chains never wait for them.
+// and sigma (two divisions by m, each a multiply by RN(1/m) and FMA
+// corrections that give the correctly rounded quotient, and a square root
+// per window) and write them out, so the chains never wait for them.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -53,6 +54,7 @@ __global__ void __launch_bounds__(kMvmeanThreads) k_mvmean(const double* __restr
         const int k0 = t * kTile, cnt = min(kTile, mk - k0);
         const int b = t & 1;
         const double dm = (double)m;
+        const double invm = ddiv(1.0, dm);  // S / m by the reciprocal method (correctly rounded)
         const double qnan = dnan();
         for (int idx = tid - 32; idx < 32 * kTile; idx += kMvmeanThreads - 32) {
             const int r = idx / kTile, x = idx % kTile;  // segment s0 + r, point k0 + x
@@ -65,8 +67,8 @@ __global__ void __launch_bounds__(kMvmeanThreads) k_mvmean(const double* __restr
                     mean = bad ? qnan : 0.0;
                     sd = bad ? qnan : 1.0;
                 } else {
-                    mean = bad ? qnan : ddiv(S1[o], dm);
-                    sd = bad ? qnan : dsqrt(dsub(ddiv(S2[o], dm), dmul(mean, mean)));
+                    mean = bad ? qnan : zdiv_i(S1[o], dm, invm, true);
+                    sd = bad ? qnan : dsqrt(dsub(zdiv_i(S2[o], dm, invm, true), dmul(mean, mean)));
                 }
                 const long long w = sr * kml + (k0 + x - m + 1);
                 mu[w] = mean;

@@ -15,11 +15,15 @@ point) and a grow-only device workspace whose size is the largest request it
 has served.  `footprint(n, m, mode)` bounds a request's workspace from the
 engine's buffers (window statistics, segment envelopes, the target's forward
 windows, the candidate lists of the LB/GLB/DP stages, the result and sort
-buffers).  A request is admitted when its target's series plus the larger of
-its current workspace and the request's footprint, together with every other
-target's series and workspace, stays within the budget; otherwise it fails
-with FSMELD_E_NOMEM and nothing else is disturbed.  The engine enforces the
-same limit itself (`set_workspace_limit`).
+buffers).  A request is admitted when its footprint alone fits in the room
+its target has: the budget less every other target's series and the
+workspace its engine holds, and less its own series.  When it does not, the
+other targets' engines (idle while this group runs) release their workspace
+first; a request that still does not fit fails with FSMELD_E_NOMEM and
+nothing else is disturbed.  The admitted requests of a group share the room:
+the engine caps its workspace there (`set_workspace_limit`, counted over its
+batch workers too) and runs a query refused for workspace while the others
+held theirs again alone, once their buffers are released.
 """
 from __future__ import annotations
 
@@ -120,8 +124,25 @@ class Server:
         self._thread.start()
 
     # ---------------------------------------------------------------- targets
+    @staticmethod
+    def _held(t: _Target) -> int:
+        """Workspace bytes a target's engine holds: the engine's own count when
+        it keeps one (its batch workers included), else the footprint of the
+        largest request it has served."""
+        held = getattr(t.engine, "workspace_bytes", None)
+        return max(t.workspace, int(held())) if held is not None else t.workspace
+
     def _used(self, exclude: str | None = None) -> int:
-        return sum(8 * t.n + t.workspace for name, t in self._targets.items() if name != exclude)
+        return sum(8 * t.n + self._held(t) for name, t in self._targets.items() if name != exclude)
+
+    def _release_others(self, name: str) -> None:
+        """Free the workspace of every other target's engine (idle while this
+        worker serves `name`); the caller holds the targets lock."""
+        for other, t in self._targets.items():
+            rel = getattr(t.engine, "release_workspace", None)
+            if other != name and rel is not None:
+                rel()
+                t.workspace = 0
 
     def add_target(self, name: str, target) -> None:
         t = np.ascontiguousarray(target, dtype=np.float64)
@@ -199,11 +220,16 @@ class Server:
                     r.future.set_exception(KeyError(f"unknown target {name!r}"))
                 return
             room = self.budget - self._used(exclude=name) - 8 * tgt.n
+            # each request must fit alone; several of them share the room as
+            # far as it goes (the engine runs a query refused for workspace
+            # again alone once the others' buffers are released)
+            fps = [footprint(tgt.n, r.spec["m"], mode, 1) if r.spec["m"] <= tgt.n else 0 for r in reqs]
+            if fps and max(fps) > room:
+                self._release_others(name)
+                room = self.budget - self._used(exclude=name) - 8 * tgt.n
         admitted = []
-        conc = min(CONCURRENCY, len(reqs))
-        for r in reqs:
-            fp = footprint(tgt.n, r.spec["m"], mode, conc) if r.spec["m"] <= tgt.n else 0
-            if max(tgt.workspace, fp) > room:
+        for r, fp in zip(reqs, fps):
+            if fp > room:
                 r.future.set_exception(ServerError(E_NOMEM, "request does not fit in the HBM budget"))
             else:
                 admitted.append((r, fp))

@@ -158,8 +158,19 @@ int fsmeld_set_lb_form(fsmeld_ctx* ctx, int form);
  * binding loads into every context. */
 int fsmeld_set_tuning(fsmeld_ctx* ctx, const char* table);
 
-/* Cap on device workspace bytes (0 = no cap); exceeding it -> FSMELD_E_NOMEM. */
+/* Cap on device workspace bytes (0 = no cap); exceeding it -> FSMELD_E_NOMEM.
+ * The cap covers the context and the worker contexts of its batches together.
+ * A batch query refused for workspace while the other queries of its batch
+ * held theirs is run again alone, after the workers' buffers are released;
+ * only a query that does not fit alone fails with FSMELD_E_NOMEM. */
 int fsmeld_set_workspace_limit(fsmeld_ctx* ctx, int64_t bytes);
+/* Device workspace bytes the context and its workers hold now (buffers grow
+ * to the largest query served and are kept for the next call). */
+int64_t fsmeld_workspace_bytes(fsmeld_ctx* ctx);
+/* Frees the workspace of the context and its workers (the target stays
+ * resident); the next call allocates what it needs again.  Waits for the
+ * context's work in flight. */
+int fsmeld_release_workspace(fsmeld_ctx* ctx);
 /* Number of CUDA kernel launches issued by this context so far. */
 int64_t fsmeld_kernel_launches(const fsmeld_ctx* ctx);
 /* Per-stage device timing (no counterpart in the reference): when on, each
