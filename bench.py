@@ -767,6 +767,7 @@ def workload_c5(args):
         if not done.wait(timeout=600):
             raise RuntimeError("c5: requests still pending after 600 s")
         span = time.perf_counter() - t_start
+        budget_gb = srv.budget / 1e9
     failed = sum(1 for a in answers if a is None)
     # answers in the mix against the same requests alone
     checked = 0
@@ -790,7 +791,8 @@ def workload_c5(args):
             "latency_ms": {"p50": round(float(np.percentile(lat_ms, 50)), 2),
                            "p99": round(float(np.percentile(lat_ms, 99)), 2),
                            "max": round(float(lat_ms.max()), 2)},
-            "failed": failed, "failures": errors, "answers_checked_against_alone": checked,
+            "failed": failed, "failures": errors, "hbm_budget_gb": round(budget_gb, 1),
+            "answers_checked_against_alone": checked,
             "cutoff_precompute_s": round(t_pre, 1)}
     print(json.dumps(line))
     return 0

@@ -279,8 +279,14 @@ static int buf(fsmeld_ctx* c, const std::string& name, size_t bytes, void** out)
     if (b.bytes < bytes) {
         if (b.p) { cudaFree(b.p); b.p = nullptr; b.bytes = 0; }
         const size_t want = bytes + bytes / 8;
-        if (root->ws_limit > 0 && (long long)(ws_family_total(root) + want) > root->ws_limit)
-            return fail(FSMELD_E_NOMEM, "Device workspace budget exceeded.");
+        const size_t held = ws_family_total(root);
+        if (root->ws_limit > 0 && (long long)(held + want) > root->ws_limit) {
+            char msg[256];
+            snprintf(msg, sizeof(msg),
+                     "Device workspace budget exceeded: %.2f GB held, %.2f GB more for '%s', limit %.2f GB.",
+                     held / 1e9, want / 1e9, name.c_str(), root->ws_limit / 1e9);
+            return fail(FSMELD_E_NOMEM, msg);
+        }
         cudaError_t e = cudaMalloc(&b.p, want);
         if (e != cudaSuccess) { b.p = nullptr; return cuda_fail(e, "cudaMalloc", __FILE__, __LINE__); }
         b.bytes = want;
@@ -1162,6 +1168,22 @@ static int run_search_gemm(fsmeld_ctx* c, const Geom& g0, Stats& st, const std::
         gj.zout = zq; gj.zstride = g0.S * g0.kml;
         gj.bits = topk ? nullptr : dbits; gj.bit_words = words;
         gj.nsurv = dcnt; gj.nvalid = dcnt + nq; gj.err = (unsigned*)(dcnt + 2 * nq);
+        // the group's window masks, once for all tiles
+        {
+            const int mw = gemm_mask_words(g0.m_k, g0.kml, m);
+            unsigned* dmask;
+            if ((r = bufT(c, "gemmMask", 2 * (size_t)g0.S * mw, &dmask))) return r;
+            gj.mask_l = dmask;
+            gj.mask_u = dmask + (size_t)g0.S * mw;
+            gj.mask_words = mw;
+            const long long warps = g0.S * (long long)mw;
+            const unsigned mgrid = (unsigned)std::max<long long>(1, std::min<long long>((warps + 7) / 8,
+                                                                                         (long long)c->sm_count * 16));
+            prof_begin(c, ST_GEMM);
+            k_gemm_masks<<<mgrid, 256, 0, c->stream>>>(g0, st.Ln, st.Un, th.t_l, th.t_u, dmask,
+                                                       dmask + (size_t)g0.S * mw, mw);
+            LAUNCH_CHECK(c);
+        }
         const void* kf = lbgemm_kernel(NQ);
         const size_t smem = lbgemm_smem_bytes(NQ, m);
         if ((r = allow_smem(c, kf, smem))) return r;
@@ -1427,7 +1449,10 @@ static int run_tasks_parallel(fsmeld_ctx* c, std::vector<QueryRun>& runs, const 
     bool nomem = false;
     for (size_t k = 0; k < order.size(); ++k) nomem = nomem || (*status)[order[k]] == FSMELD_E_NOMEM;
     if (nomem && !cuda_dead.load()) {
-        for (int t = 0; t < conc; ++t) release_bufs(ws[t]);
+        // every task computes its own statistics on its worker, so nothing the
+        // context itself holds is needed here either
+        release_bufs(c);
+        for (fsmeld_ctx* w : c->workers) release_bufs(w);
         for (size_t ti = 0; ti < tasks.size() && !cuda_dead.load(); ++ti) {
             bool any = false;
             for (size_t k = tasks[ti].first; k < tasks[ti].second; ++k)
@@ -1556,7 +1581,7 @@ int run_batch(fsmeld_ctx* c, std::vector<QueryRun>& runs, std::vector<int>* stat
                 dead = dead || (*status)[k] == FSMELD_E_CUDA;
             }
             if (nomem && !dead) {
-                for (int t = 0; t < conc; ++t) release_bufs(ws[t]);
+                for (fsmeld_ctx* w : c->workers) release_bufs(w);
                 for (size_t k : rest) {
                     if ((*status)[k] != FSMELD_E_NOMEM) continue;
                     const int q = run_query(c, runs[k], g, st, have_env);

@@ -24,8 +24,10 @@
 // query to make it tight; here one pair serves the whole group).
 //
 // Tiles: a CTA of 128 threads takes one (segment, 128-window tile) at a
-// time.  Per 64-wide K chunk, the threads write the A tiles of both sides
-// from a bit mask of the tile's span (g for positions j0 .. j0+127+m) and
+// time.  The group's window masks g (one bit per segment position and side)
+// are computed once before the product (k_gemm_masks, one ballot per 32
+// positions).  Per 64-wide K chunk, the threads write the A tiles of both
+// sides from the mask words of the tile's span (positions j0 .. j0+127+m) and
 // copy the chunk of B (pre-arranged on the host in the operand layout), in
 // the canonical no-swizzle K-major layout (8-row x 16-byte core matrices:
 // rows 16 B apart, row groups SBO = 128 B apart, 8-element K groups LBO
@@ -183,17 +185,14 @@ __global__ void __launch_bounds__(kGemmThreads) k_lbgemm(Geom g, GemmJob job) {
     for (long long it = blockIdx.x; it < items && !failed; it += gridDim.x) {
         const long long s = it / tiles;
         const int j0 = (int)(it - s * tiles) * 128;
-        const double* Ln = job.Ln + s * mk;
-        const double* Un = job.Un + s * mk;
-        // masks of the tile's span: positions j0 .. j0 + 128 + kpad (0 past the segment)
-        for (int base = warp * 32; base < words * 64; base += kGemmThreads) {
-            const int p = j0 + base + lane;
-            const bool in = p < mk;
-            const unsigned bl = __ballot_sync(0xffffffffu, in && Ln[in ? p : 0] >= job.t_l);
-            const unsigned bu = __ballot_sync(0xffffffffu, in && Un[in ? p : 0] <= job.t_u);
-            if (lane == 0) {
-                ((unsigned*)GLb)[base >> 5] = bl;
-                ((unsigned*)GUb)[base >> 5] = bu;
+        // masks of the tile's span: positions j0 .. j0 + 128 + kpad (0 past the
+        // segment), copied from the group's precomputed mask words
+        {
+            const unsigned* ml = job.mask_l + s * (long long)job.mask_words + (j0 >> 5);
+            const unsigned* mu = job.mask_u + s * (long long)job.mask_words + (j0 >> 5);
+            for (int i = tid; i < 2 * words; i += kGemmThreads) {
+                ((unsigned*)GLb)[i] = ml[i];
+                ((unsigned*)GUb)[i] = mu[i];
             }
         }
         __syncthreads();
@@ -301,6 +300,37 @@ __global__ void __launch_bounds__(kGemmThreads) k_lbgemm(Geom g, GemmJob job) {
     if (failed) mbar_wait(bar, phase ^ 1);  // let issued MMAs drain (bounded) before freeing TMEM
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
+}
+
+int gemm_mask_words(int m_k, int kml, int m) {
+    const int kpad = (m + kKChunk - 1) / kKChunk * kKChunk;
+    const int words = (128 + kpad + 63) / 64 + 2;  // 64-bit words a tile reads (k_lbgemm)
+    const int tiles = (kml + 127) / 128;
+    const int need = (tiles - 1) * 4 + 2 * words;   // 32-bit words up to the last tile's span
+    const int cover = (m_k + 31) / 32;
+    return (need > cover ? need : cover) + 1;
+}
+
+// One warp per 32 positions: the ballot of the threshold tests is the word.
+__global__ void __launch_bounds__(256) k_gemm_masks(Geom g, const double* __restrict__ Ln,
+                                                    const double* __restrict__ Un, double t_l, double t_u,
+                                                    unsigned* __restrict__ mask_l, unsigned* __restrict__ mask_u,
+                                                    int words) {
+    const int lane = threadIdx.x & 31;
+    const long long total = g.S * (long long)words;
+    const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long it = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < total; it += nwarps) {
+        const long long s = it / words;
+        const int p = (int)(it - s * words) * 32 + lane;
+        const bool in = p < g.m_k;
+        const long long o = s * (long long)g.m_k + (in ? p : 0);
+        const unsigned bl = __ballot_sync(0xffffffffu, in && Ln[o] >= t_l);
+        const unsigned bu = __ballot_sync(0xffffffffu, in && Un[o] <= t_u);
+        if (lane == 0) {
+            mask_l[it] = bl;
+            mask_u[it] = bu;
+        }
+    }
 }
 
 // survivor bit mask -> list of window indices (ascending within a block of

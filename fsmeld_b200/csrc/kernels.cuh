@@ -97,9 +97,17 @@ struct GemmJob {
     unsigned long long* nsurv;  // [nq]
     unsigned long long* nvalid; // [nq]
     unsigned int* err;          // set when a bounded wait gave up
+    const unsigned* mask_l;     // window masks g of the group (k_gemm_masks): [S][mask_words] 32-bit words,
+    const unsigned* mask_u;     // bit p of a segment = position p (0 at and past m_k)
+    int mask_words;
 };
 template <int NQ>
 __global__ void k_lbgemm(Geom g, GemmJob job);
+// bit p of segment s: Ln[s][p] >= t_l (mask_l), Un[s][p] <= t_u (mask_u); 0 for p >= m_k
+__global__ void k_gemm_masks(Geom g, const double* __restrict__ Ln, const double* __restrict__ Un, double t_l,
+                             double t_u, unsigned* __restrict__ mask_l, unsigned* __restrict__ mask_u, int words);
+// 32-bit mask words per segment: the positions every tile of the segment reads
+int gemm_mask_words(int m_k, int kml, int m);
 const void* lbgemm_kernel(int nq_pad);  // NQ in {16, 32, 64, 128}
 __global__ void k_bits_to_list(const unsigned* __restrict__ bits, long long words, long long* __restrict__ out,
                                long long cap, unsigned long long* __restrict__ n);
