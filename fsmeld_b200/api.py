@@ -81,6 +81,7 @@ def lib():
             "fsmeld_strerror": (C.c_char_p, [C.c_int]),
             "fsmeld_set_workspace_limit": (C.c_int, [ctxp, C.c_int64]),
             "fsmeld_workspace_bytes": (C.c_int64, [ctxp]),
+            "fsmeld_target_device": (C.c_void_p, [ctxp]),
             "fsmeld_release_workspace": (C.c_int, [ctxp]),
             "fsmeld_set_concurrency": (C.c_int, [ctxp, C.c_int]),
             "fsmeld_set_normalization": (C.c_int, [ctxp, C.c_int]),
@@ -222,6 +223,10 @@ class Engine:
 
     def set_workspace_limit(self, nbytes):
         _check(lib().fsmeld_set_workspace_limit(self._ctx, int(nbytes)), self._ctx)
+
+    def target_device_ptr(self):
+        """Device address of the resident target (for engines that borrow it)."""
+        return int(lib().fsmeld_target_device(self._ctx))
 
     def workspace_bytes(self):
         """Device workspace bytes this engine holds now (its batch workers included)."""

@@ -1540,7 +1540,13 @@ int run_batch(fsmeld_ctx* c, std::vector<QueryRun>& runs, std::vector<int>* stat
         const int conc = std::min(std::max(1, c->concurrency), std::max(1, nq));
         if (conc <= 1) {
             for (size_t k : rest) {
-                const int q = run_query(c, runs[k], g, st, have_env);
+                int q = run_query(c, runs[k], g, st, have_env);
+                if (q == FSMELD_E_NOMEM && !c->workers.empty()) {
+                    // the buffers an earlier batch's workers kept may be what is
+                    // missing: release them and run the query again
+                    for (fsmeld_ctx* w : c->workers) release_bufs(w);
+                    q = run_query(c, runs[k], g, st, have_env);
+                }
                 (*status)[k] = q;
                 if (q && !first_err) first_err = q;
                 if (q == FSMELD_E_CUDA) break;
@@ -1714,6 +1720,8 @@ int fsmeld_close(fsmeld_ctx* c) {
 }
 
 int64_t fsmeld_target_length(const fsmeld_ctx* c) { return c ? c->n : 0; }
+
+const double* fsmeld_target_device(const fsmeld_ctx* c) { return c ? c->d_target : nullptr; }
 
 int fsmeld_set_normalization(fsmeld_ctx* c, int mode) {
     if (!c || (mode != FSMELD_NORM_ZSCORE && mode != FSMELD_NORM_RAW))

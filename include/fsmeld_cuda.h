@@ -107,6 +107,10 @@ int fsmeld_load(fsmeld_ctx* ctx, const double* host_target, int64_t n);
 int fsmeld_open_device(int device, const double* device_target, int64_t n, fsmeld_ctx** out);
 int fsmeld_close(fsmeld_ctx* ctx);
 int64_t fsmeld_target_length(const fsmeld_ctx* ctx);
+/* Device address of the context's resident target (owned or borrowed), for
+ * opening further contexts over the same series with fsmeld_open_device
+ * (they must be closed before the owner).  No counterpart in the reference. */
+const double* fsmeld_target_device(const fsmeld_ctx* ctx);
 const char* fsmeld_last_error(const fsmeld_ctx* ctx);
 const char* fsmeld_strerror(int status);
 /* Batched calls (fsmeld_batch): the queries of one (m, w) group run

@@ -1,8 +1,9 @@
 """The serving loop's host logic (fsmeld_b200.serve) with a stand-in engine:
 requests are grouped by target and mode in arrival order, every answer
 reaches its own future, admission by HBM footprint rejects what does not fit
-and serves the rest, and a result larger than the batch buffer is fetched
-alone."""
+and serves the rest, a result larger than the batch buffer is fetched alone,
+a long request holds one slot while the others keep serving, and a batch
+whose room is taken by a running one waits for it instead of failing."""
 import threading
 import time
 
@@ -24,7 +25,7 @@ class FakeEngine:
     def set_workspace_limit(self, b):
         self.limit = b
 
-    def batch(self, mode, specs):
+    def batch(self, mode, specs, capacity=1 << 14):
         if self.gate is not None:
             self.gate.wait()
         self.log.append((mode, len(specs)))
@@ -54,7 +55,7 @@ def _q(i, m=32):
 def test_routing_and_grouping():
     log = []
     gate = threading.Event()
-    srv = Server(budget_bytes=1 << 40, max_batch=64, engine_factory=lambda t: FakeEngine(t, log, gate))
+    srv = Server(budget_bytes=1 << 40, max_batch=64, slots=1, engine_factory=lambda t: FakeEngine(t, log, gate))
     try:
         srv.add_target("a", np.zeros(4096))
         srv.add_target("b", np.zeros(8192))
@@ -91,7 +92,7 @@ def test_admission_by_footprint():
     big = footprint(n, 4096, "search")
     assert big > small + 4 * n
     # room for target a, its largest small request and half of another series
-    srv = Server(budget_bytes=8 * n + small + 4 * n, engine_factory=lambda t: FakeEngine(t, log))
+    srv = Server(budget_bytes=8 * n + small + 4 * n, slots=1, engine_factory=lambda t: FakeEngine(t, log))
     try:
         srv.add_target("a", np.zeros(n))
         ok = srv.submit("a", "search", _q(1), 32, "dtw", 3, cutoff=1.0)
@@ -118,4 +119,61 @@ def test_large_result_fetched_alone_and_bad_requests():
         with pytest.raises(ValueError):
             srv.submit("a", "cutoff", _q(3), 32, "dtw", 3, cutoff=1.0)
     finally:
+        srv.close()
+
+
+class SlowEngine(FakeEngine):
+    """Blocks the batches whose first query has cutoff 7.0 until `gate` is set."""
+
+    def __init__(self, t, log, gate, started):
+        super().__init__(t, log)
+        self.slow_gate = gate
+        self.started = started
+
+    def batch(self, mode, specs, capacity=1 << 14):
+        self.started.append(tuple(s.get("cutoff") for s in specs))
+        if specs[0].get("cutoff") == 7.0:
+            self.slow_gate.wait(timeout=20)
+        return super().batch(mode, specs, capacity)
+
+
+def test_long_request_holds_one_slot():
+    log, started = [], []
+    gate = threading.Event()
+    srv = Server(budget_bytes=1 << 40, slots=2, engine_factory=lambda t: SlowEngine(t, log, gate, started))
+    try:
+        srv.add_target("a", np.zeros(4096))
+        slow = srv.submit("a", "search", _q(1), 32, "dtw", 3, cutoff=7.0)
+        time.sleep(0.2)
+        fast = srv.submit("a", "search", _q(2), 32, "dtw", 3, cutoff=1.0)
+        fast.result(timeout=10)  # served by the second slot while the first is held
+        assert not slow.done()
+        gate.set()
+        slow.result(timeout=10)
+    finally:
+        gate.set()
+        srv.close()
+
+
+def test_batch_waits_for_room_held_by_a_running_one():
+    log, started = [], []
+    gate = threading.Event()
+    n = 1 << 16
+    fp = footprint(n, 32, "search")
+    # room for the series and one request's workspace: the second request
+    # waits until the first one's slot is done, then runs (no FSMELD_E_NOMEM)
+    srv = Server(budget_bytes=8 * n + fp + fp // 2, slots=2,
+                 engine_factory=lambda t: SlowEngine(t, log, gate, started))
+    try:
+        srv.add_target("a", np.zeros(n))
+        first = srv.submit("a", "search", _q(1), 32, "dtw", 3, cutoff=7.0)
+        time.sleep(0.2)
+        second = srv.submit("a", "search", _q(2), 32, "dtw", 3, cutoff=1.0)
+        time.sleep(0.3)
+        assert not second.done() and len(started) == 1
+        gate.set()
+        first.result(timeout=10)
+        assert second.result(timeout=10)[0].shape == (1,)
+    finally:
+        gate.set()
         srv.close()
