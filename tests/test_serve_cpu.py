@@ -177,3 +177,52 @@ def test_batch_waits_for_room_held_by_a_running_one():
     finally:
         gate.set()
         srv.close()
+
+
+class HoldingEngine(FakeEngine):
+    """Keeps `held` bytes after a batch (its workers' buffers); a request run
+    alone fails with FSMELD_E_NOMEM until that workspace is released."""
+
+    def __init__(self, t, log):
+        super().__init__(t, log)
+        self.held = 0
+        self.released = 0
+
+    def workspace_bytes(self):
+        return self.held
+
+    def release_workspace(self):
+        self.held = 0
+        self.released += 1
+
+    def batch(self, mode, specs, capacity=1 << 14):
+        out = super().batch(mode, specs, capacity)
+        self.held = 1 << 30
+        return out
+
+    def search(self, q, m, cutoff, metric, w, arg, exclude=(-1, -1)):
+        if self.held:
+            err = RuntimeError("Device workspace budget exceeded")
+            err.status = E_NOMEM
+            raise err
+        return super().search(q, m, cutoff, metric, w, arg, exclude)
+
+
+def test_large_result_alone_after_release():
+    log = []
+    engines = []
+
+    def factory(t):
+        e = HoldingEngine(t, log)
+        engines.append(e)
+        return e
+
+    srv = Server(budget_bytes=1 << 40, slots=1, engine_factory=factory)
+    try:
+        srv.add_target("a", np.zeros(4096))
+        # cutoff 99.0: the stand-in reports more matches than the batch buffer
+        idx, cnt = srv.submit("a", "search", _q(3), 32, "dtw", 3, cutoff=99.0).result(timeout=10)
+        assert list(idx) == [0, 1, 2, 3, 4]
+        assert engines[0].released == 1
+    finally:
+        srv.close()
